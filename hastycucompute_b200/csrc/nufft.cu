@@ -1,0 +1,923 @@
+// NUFFT type 1 / type 2 on B200: bin sort, tile-owned spreading, point-gather interpolation,
+// and the pruned FFT passes with the deapodisation fused into the first / last pass.
+//
+// Algorithm (the restated cufinufft pipeline, cpp/corelib/lib/fft/nufft.cppm:205-250 calls):
+//   type 1: g = spread(c)  ->  G = FFT_sign(g) over the fine grid  ->  f[k] = G[k mod nf]/phihat(k)
+//   type 2: G[k mod nf] = f[k]/phihat(k)  ->  g = FFT_sign(G)  ->  c_j = interp(g, x_j)
+// with phi the Kaiser-Bessel kernel and phihat its Fourier transform.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "nufft.cuh"
+#include "ops.cuh"
+
+namespace hb {
+
+// ---------------------------------------------------------------------------------------------
+// small helpers
+
+static bool smooth235(int n) {
+    for (int r : {2, 3, 5})
+        while (n % r == 0 && n > 1) n /= r;
+    return n == 1;
+}
+
+static int fine_size(int64_t N, double sigma, int w, int T) {
+    if (N <= 1) return 1;
+    int64_t lo = (int64_t)std::ceil(sigma * (double)N - 1e-9);
+    lo = std::max<int64_t>(lo, 2 * w);
+    lo = std::max<int64_t>(lo, T);
+    for (int64_t n = lo;; ++n)
+        if (n % T == 0 && smooth235((int)n)) return (int)n;
+}
+
+static int pow2ceil(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// Coil chunk (power of two, <= 32) a spread CTA accumulates at once.
+static int spread_cc(const GridGeom& g) {
+    const int cells = g.T[0] * g.T[1] * g.T[2];
+    int cmax = 32;
+    while (cmax > 1 && (size_t)cells * cmax * 8 > 131072) cmax >>= 1;
+    return std::min(pow2ceil(g.C), cmax);
+}
+
+// ---------------------------------------------------------------------------------------------
+// setpts kernels
+
+struct FoldArgs {
+    const float* c[3];  // caller coordinate per internal axis (nullptr on unit axes)
+    float* u[3];        // unsorted fine coordinates
+    int* binid;
+    int* rank;
+    int* count;
+    int* err;
+    int nf[3], T[3], nb[3];
+    float scale[3];
+    float hw;
+    int64_t M;
+};
+
+__device__ __forceinline__ float fold_fine(float x, float scale, int nf) {
+    float u = __fmul_rn(x, scale);
+    const float fnf = (float)nf;
+    const float q = floorf(__fdiv_rn(u, fnf));
+    u = __fsub_rn(u, __fmul_rn(q, fnf));
+    if (u < 0.f) u = __fadd_rn(u, fnf);
+    if (u >= fnf) u = __fsub_rn(u, fnf);
+    return u;
+}
+
+__device__ __forceinline__ int first_cell(float u, float hw, int nf) {
+    int i0 = (int)ceilf(__fsub_rn(u, hw));
+    if (i0 < 0) i0 += nf;
+    if (i0 >= nf) i0 -= nf;
+    return i0;
+}
+
+__global__ void k_fold_bin(const FoldArgs a) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= a.M) return;
+    int b[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        if (a.c[ax] == nullptr) {
+            b[ax] = 0;
+            continue;
+        }
+        float x = a.c[ax][j];
+        if (!isfinite(x)) {
+            atomicExch(a.err, 1);
+            x = 0.f;
+        }
+        const float u = fold_fine(x, a.scale[ax], a.nf[ax]);
+        a.u[ax][j] = u;
+        b[ax] = first_cell(u, a.hw, a.nf[ax]) / a.T[ax];
+    }
+    const int bin = (b[0] * a.nb[1] + b[1]) * a.nb[2] + b[2];
+    a.binid[j] = bin;
+    a.rank[j] = atomicAdd(&a.count[bin], 1);
+}
+
+__global__ void k_scatter_sorted(const float* u0, const float* u1, const float* u2, const int* binid,
+                                 const int* rank, const int* bin_start, float* s0, float* s1, float* s2,
+                                 int* perm, int64_t M) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= M) return;
+    const int s = bin_start[binid[j]] + rank[j];
+    perm[s] = (int)j;
+    if (s0) s0[s] = u0[j];
+    if (s1) s1[s] = u1[j];
+    if (s2) s2[s] = u2[j];
+}
+
+// ---- exclusive scan of ints (n + 1 outputs, out[n] = total) -------------------------------------
+constexpr int kScanBlock = 1024;
+
+__device__ __forceinline__ int block_excl_scan(int v, int* warp_sums, int& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int ws = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, ws, o);
+            if (lane >= o) ws += y;
+        }
+        warp_sums[lane] = ws;  // inclusive over warps
+    }
+    __syncthreads();
+    const int warp_off = wid > 0 ? warp_sums[wid - 1] : 0;
+    total = warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warp_off + x - v;
+}
+
+__global__ void k_scan_blocks(const int* in, int* out, int* sums, int64_t n) {
+    __shared__ int ws[32];
+    const int64_t i = (int64_t)blockIdx.x * kScanBlock + threadIdx.x;
+    const int v = i < n ? in[i] : 0;
+    int total;
+    const int ex = block_excl_scan(v, ws, total);
+    if (i < n) out[i] = ex;
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_sums(int* sums, int64_t nblocks, int* total_out) {
+    __shared__ int ws[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t base = 0; base < nblocks; base += kScanBlock) {
+        const int64_t i = base + threadIdx.x;
+        const int v = i < nblocks ? sums[i] : 0;
+        int total;
+        const int ex = block_excl_scan(v, ws, total);
+        if (i < nblocks) sums[i] = ex + carry;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void k_scan_add(int* out, const int* sums, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * kScanBlock + threadIdx.x;
+    if (i < n) out[i] += sums[blockIdx.x];
+}
+
+int exclusive_scan_int(const int* in, int* out, int64_t n, cudaStream_t s) {
+    const int64_t nb = ceil_div(std::max<int64_t>(n, 1), kScanBlock);
+    int* sums = nullptr;
+    HB_CUDA(cudaMallocAsync(&sums, sizeof(int) * nb, s));
+    k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, s>>>(in, out, sums, n);
+    k_scan_sums<<<1, kScanBlock, 0, s>>>(sums, nb, out + n);
+    k_scan_add<<<(unsigned)nb, kScanBlock, 0, s>>>(out, sums, n);
+    int st = check_launch("exclusive_scan_int");
+    HB_CUDA(cudaFreeAsync(sums, s));
+    return st;
+}
+
+// ---- spread work list --------------------------------------------------------------------------
+struct TileNbr {
+    int nb[3];
+};
+
+// Visits the (up to 8) bins whose points can reach tile (tz, ty, tx): along each axis with more
+// than one bin, the tile's own bin and the one before it (a footprint spans at most 2 tiles).
+template <class F>
+__device__ __forceinline__ void for_each_nbr_bin(const int* nb, int tz, int ty, int tx, F&& f) {
+    const int nz = nb[0] > 1 ? 2 : 1, ny = nb[1] > 1 ? 2 : 1, nx = nb[2] > 1 ? 2 : 1;
+    for (int dz = 0; dz < nz; ++dz) {
+        const int bz = (tz - dz + nb[0]) % nb[0];
+        for (int dy = 0; dy < ny; ++dy) {
+            const int by = (ty - dy + nb[1]) % nb[1];
+            for (int dx = 0; dx < nx; ++dx) {
+                const int bx = (tx - dx + nb[2]) % nb[2];
+                f((bz * nb[1] + by) * nb[2] + bx);
+            }
+        }
+    }
+}
+
+__global__ void k_tile_extra_count(const int* bin_start, TileNbr t, int64_t ntiles, int maxp, int* extra_cnt) {
+    const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= ntiles) return;
+    const int tx = (int)(tile % t.nb[2]), ty = (int)((tile / t.nb[2]) % t.nb[1]), tz = (int)(tile / ((int64_t)t.nb[2] * t.nb[1]));
+    int64_t total = 0;
+    for_each_nbr_bin(t.nb, tz, ty, tx, [&](int bin) { total += bin_start[bin + 1] - bin_start[bin]; });
+    const int64_t nsub = total > 0 ? (total + maxp - 1) / maxp : 1;
+    extra_cnt[tile] = (int)(nsub - 1);
+}
+
+__global__ void k_tile_extra_fill(const int* extra_cnt, const int* extra_off, int64_t ntiles, int2* extra) {
+    const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= ntiles) return;
+    const int n = extra_cnt[tile], off = extra_off[tile];
+    for (int c = 0; c < n; ++c) extra[off + c] = make_int2((int)tile, c + 1);
+}
+
+// ---------------------------------------------------------------------------------------------
+// execute kernels
+
+// inT[s][c] = in[c][perm[s]]  (sorted, transforms interleaved)
+__global__ void k_permute_in(const float2* __restrict__ in, const int* __restrict__ perm, float2* __restrict__ inT,
+                             int64_t M, int C) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= M * C) return;
+    const int c = (int)(idx % C);
+    const int64_t s = idx / C;
+    inT[idx] = in[(int64_t)c * M + perm[s]];
+}
+
+struct GridArgs {
+    GridGeom g;
+    const float* su[3];
+    const int* perm;
+    const int* bin_start;
+    const float2* inT;  // spread input [M][C]
+    float2* grid;       // [nf0][nf1][nf2][C]
+    float2* out;        // interp output [C][M]
+    const int2* extra;
+    int maxp;
+    KbPoly kb;
+};
+
+constexpr int kGridThreads = 256;
+constexpr int kGridWarps = kGridThreads / 32;
+constexpr int kCoefFloats = kMaxWidth * (kMaxDeg + 1);
+constexpr int kSlotFloats = 3 * kMaxWidth;
+
+// Per point: fine coordinate -> first cell (wrapped) and the tap weights of each axis. The
+// lanes of a slot share the weight evaluation; weights land in wts[axis*kMaxWidth + d].
+__device__ __forceinline__ void point_setup(const GridArgs& a, const float* coef, int64_t s, bool valid, int lane_in_slot,
+                                            int slot_lanes, float* wts, int* i0) {
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int w = a.g.wa[ax];
+        if (w == 1) {
+            i0[ax] = 0;
+            if (lane_in_slot == 0) wts[ax * kMaxWidth] = 1.f;
+            continue;
+        }
+        const float u = valid ? a.su[ax][s] : 0.f;
+        const float hw = a.kb.hw;
+        const float v = __fsub_rn(u, hw);
+        const int ic = (int)ceilf(v);
+        const float t = __fsub_rn((float)ic, v);
+        const float sarg = fmaf(2.f, t, -1.f);
+        int iw = ic;
+        const int nf = a.g.nf[ax];
+        if (iw < 0) iw += nf;
+        if (iw >= nf) iw -= nf;
+        i0[ax] = iw;
+        for (int d = lane_in_slot; d < w; d += slot_lanes) wts[ax * kMaxWidth + d] = kb_tap(coef, a.kb.deg, d, sarg);
+    }
+}
+
+// Type-1 spreading. One CTA owns one tile of the fine grid and produces its cells exactly once
+// (plain stores for chunk 0 of every tile, atomic adds for the extra chunks of dense tiles): no
+// halo, no zero fill, no global atomics outside dense tiles. Candidate points come from the
+// tile's bin and its lower neighbours; each point is clipped to the tile. Lanes of a warp map
+// to (point slot, transform) so one point's weights serve CC transforms at once; accumulation is
+// in shared memory.
+template <int CC>
+__global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int extra_mode) {
+    extern __shared__ float sm[];
+    const GridGeom& g = a.g;
+    const int T0 = g.T[0], T1 = g.T[1], T2 = g.T[2];
+    const int cells = T0 * T1 * T2;
+    float* acc_re = sm;
+    float* acc_im = acc_re + cells * CC;
+    float* coef = acc_im + cells * CC;
+    float* wts_all = coef + kCoefFloats;
+    constexpr int NS = 32 / CC;
+    __shared__ int s_start[8], s_pref[9], s_nbin;
+
+    int tile, chunk;
+    if (extra_mode) {
+        const int2 e = a.extra[blockIdx.x];
+        tile = e.x;
+        chunk = e.y;
+    } else {
+        tile = blockIdx.x;
+        chunk = 0;
+    }
+    const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
+    const int o0 = tz * T0, o1 = ty * T1, o2 = tx * T2;
+
+    for (int i = threadIdx.x; i < kCoefFloats; i += blockDim.x) coef[i] = (&a.kb.coef[0][0])[i];
+    if (threadIdx.x == 0) {
+        int n = 0, acc = 0;
+        for_each_nbr_bin(g.nb, tz, ty, tx, [&](int bin) {
+            const int st = a.bin_start[bin];
+            s_start[n] = st;
+            s_pref[n] = acc;
+            acc += a.bin_start[bin + 1] - st;
+            ++n;
+        });
+        s_pref[n] = acc;
+        s_nbin = n;
+    }
+    __syncthreads();
+    const int total = s_pref[s_nbin];
+    const int k_begin = chunk * a.maxp;
+    const int k_end = min(total, k_begin + a.maxp);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = lane / CC, coil = lane % CC;
+    float* wts = wts_all + (warp * NS + slot) * kSlotFloats;
+
+    for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
+        for (int i = threadIdx.x; i < cells * CC; i += blockDim.x) {
+            acc_re[i] = 0.f;
+            acc_im[i] = 0.f;
+        }
+        __syncthreads();
+        const bool coil_ok = (cc0 + coil) < g.C;
+        for (int base = k_begin + warp * NS; base < k_end; base += kGridWarps * NS) {
+            const int k = base + slot;
+            const bool valid = k < k_end;
+            int64_t s = 0;
+            if (valid) {
+                int b = 0;
+                while (b + 1 < s_nbin && s_pref[b + 1] <= k) ++b;
+                s = s_start[b] + (k - s_pref[b]);
+            }
+            int i0[3];
+            point_setup(a, coef, s, valid, coil, CC, wts, i0);
+            __syncwarp();
+            if (valid && coil_ok) {
+                const float2 v = a.inT[s * g.C + cc0 + coil];
+                int r0 = i0[0] - o0, r1 = i0[1] - o1, r2 = i0[2] - o2;
+                if (r0 < 0) r0 += g.nf[0];
+                if (r1 < 0) r1 += g.nf[1];
+                if (r2 < 0) r2 += g.nf[2];
+                for (int dz = 0; dz < g.wa[0]; ++dz) {
+                    int cz = r0 + dz;
+                    if (cz >= g.nf[0]) cz -= g.nf[0];
+                    if (cz >= T0) continue;
+                    const float wz = wts[dz];
+                    for (int dy = 0; dy < g.wa[1]; ++dy) {
+                        int cy = r1 + dy;
+                        if (cy >= g.nf[1]) cy -= g.nf[1];
+                        if (cy >= T1) continue;
+                        const float wzy = wz * wts[kMaxWidth + dy];
+                        const int rowc = (cz * T1 + cy) * T2;
+                        for (int dx = 0; dx < g.wa[2]; ++dx) {
+                            int cx = r2 + dx;
+                            if (cx >= g.nf[2]) cx -= g.nf[2];
+                            if (cx >= T2) continue;
+                            const float wgt = wzy * wts[2 * kMaxWidth + dx];
+                            const int ci = (rowc + cx) * CC + coil;
+                            atomicAdd(&acc_re[ci], wgt * v.x);
+                            atomicAdd(&acc_im[ci], wgt * v.y);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < cells * CC; i += blockDim.x) {
+            const int c = i % CC, cell = i / CC;
+            if (cc0 + c >= g.C) continue;
+            const int cx = cell % T2, cy = (cell / T2) % T1, cz = cell / (T1 * T2);
+            const int64_t gi = ((int64_t)(o0 + cz) * g.nf[1] + (o1 + cy)) * g.nf[2] + (o2 + cx);
+            float2* dst = a.grid + gi * g.C + cc0 + c;
+            if (extra_mode) {
+                atomicAdd(&dst->x, acc_re[i]);
+                atomicAdd(&dst->y, acc_im[i]);
+            } else {
+                *dst = make_float2(acc_re[i], acc_im[i]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Type-2 interpolation: lanes of a warp map to (point slot, transform); each lane gathers its
+// transform's w^d taps (the CC values of a cell are contiguous), then scatters to the caller's
+// point order.
+template <int CC>
+__global__ void __launch_bounds__(kGridThreads) k_interp(const GridArgs a) {
+    extern __shared__ float sm[];
+    constexpr int NS = 32 / CC;
+    float* coef = sm;
+    float* wts_all = coef + kCoefFloats;
+    const GridGeom& g = a.g;
+    for (int i = threadIdx.x; i < kCoefFloats; i += blockDim.x) coef[i] = (&a.kb.coef[0][0])[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = lane / CC, coil = lane % CC;
+    float* wts = wts_all + (warp * NS + slot) * kSlotFloats;
+    const int64_t gwarp = (int64_t)blockIdx.x * kGridWarps + warp;
+    const int64_t nwarps = (int64_t)gridDim.x * kGridWarps;
+    const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+    for (int64_t base = gwarp * NS; base < g.M; base += nwarps * NS) {
+        const int64_t s = base + slot;
+        const bool valid = s < g.M;
+        int i0[3];
+        point_setup(a, coef, s, valid, coil, CC, wts, i0);
+        __syncwarp();
+        if (valid) {
+            const int pj = a.perm[s];
+            for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
+                if (cc0 + coil >= g.C) break;
+                float ar = 0.f, ai = 0.f;
+                for (int dz = 0; dz < g.wa[0]; ++dz) {
+                    int gz = i0[0] + dz;
+                    if (gz >= nf0) gz -= nf0;
+                    const float wz = wts[dz];
+                    for (int dy = 0; dy < g.wa[1]; ++dy) {
+                        int gy = i0[1] + dy;
+                        if (gy >= nf1) gy -= nf1;
+                        const float wzy = wz * wts[kMaxWidth + dy];
+                        const int64_t row = ((int64_t)gz * nf1 + gy) * nf2;
+                        for (int dx = 0; dx < g.wa[2]; ++dx) {
+                            int gx = i0[2] + dx;
+                            if (gx >= nf2) gx -= nf2;
+                            const float wgt = wzy * wts[2 * kMaxWidth + dx];
+                            const float2 v = a.grid[(row + gx) * g.C + cc0 + coil];
+                            ar = fmaf(wgt, v.x, ar);
+                            ai = fmaf(wgt, v.y, ai);
+                        }
+                    }
+                }
+                a.out[(int64_t)(cc0 + coil) * g.M + pj] = make_float2(ar, ai);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---- x-axis passes between the caller's [C][N..] modes and the interleaved buffers ----------
+// Load modes f[e][a][l] (a = row over axes 0,1; l = axis 2) pre-scaled by 1/phihat.
+struct OpModesIn {
+    static constexpr bool kLoadLFast = true;
+    static constexpr bool kFusedK = false;
+    static constexpr bool kChunkLoop = false;
+    const float2* f;
+    float2* dst;  // [rows][nf2][C]
+    const float* d0;
+    const float* d1;
+    const float* d2;
+    int64_t N1, N2, nm;  // modes of axis 1, 2; modes per transform
+    int64_t d_a, d_l;
+    __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
+        const float sc = d0[a / N1] * d1[a % N1] * d2[l];
+        return cscale(f[e * nm + a * N2 + l], sc);
+    }
+    __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
+                                                float2*) const {
+        float2* d = dst;
+        const int64_t da = d_a, dl = d_l;
+        for_each_output<false>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) { d[a * da + (int64_t)o * dl + e] = v; });
+    }
+    __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
+};
+
+// Store modes f[e][a][o] scaled by 1/phihat from the interleaved buffer.
+struct OpModesOut {
+    static constexpr bool kLoadLFast = false;
+    static constexpr bool kFusedK = false;
+    static constexpr bool kChunkLoop = false;
+    const float2* src;  // [rows][nf2][C]
+    float2* f;
+    const float* d0;
+    const float* d1;
+    const float* d2;
+    int64_t N1, N2, nm;
+    int64_t s_a, s_l;
+    __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
+    __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
+                                                float2*) const {
+        for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) {
+            const float sc = d0[a / N1] * d1[a % N1] * d2[o];
+            f[e * nm + a * N2 + o] = cscale(v, sc);
+        });
+    }
+    __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
+};
+
+// ---------------------------------------------------------------------------------------------
+// plan lifecycle
+
+static int dev_alloc(NufftPlan* p, void** ptr, size_t bytes, const char* what) {
+    cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        set_error(std::string("cudaMalloc(") + what + ", " + std::to_string(bytes) + " bytes) failed: " +
+                  cudaGetErrorString(e));
+        return HB_ERR_ALLOC;
+    }
+    p->device_bytes += bytes;
+    return HB_OK;
+}
+
+int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, int ntransf, float tol, int width,
+              double upsampfac, int method) {
+    HB_REQUIRE(type == 1 || type == 2, HB_ERR_INVALID_ARG, "nufft type must be 1 or 2");
+    HB_REQUIRE(dim >= 1 && dim <= 3, HB_ERR_INVALID_ARG, "dim must be 1, 2 or 3");
+    HB_REQUIRE(nmodes != nullptr, HB_ERR_INVALID_ARG, "nmodes is null");
+    HB_REQUIRE(ntransf >= 1, HB_ERR_INVALID_ARG, "ntransf must be >= 1");
+    HB_REQUIRE(method >= 0 && method <= 3, HB_ERR_INVALID_ARG, "invalid method");
+    HB_REQUIRE(sign == 0 || sign == 1 || sign == -1, HB_ERR_INVALID_ARG, "sign must be -1, 0 or +1");
+    p->type = type;
+    p->sign = sign != 0 ? sign : (type == 1 ? 1 : -1);
+    p->method = method;
+    p->sigma = upsampfac > 0 ? upsampfac : 2.0;
+    HB_REQUIRE(p->sigma >= 1.1 && p->sigma <= 4.0, HB_ERR_INVALID_ARG, "upsampfac must be in [1.1, 4]");
+    int w = width;
+    if (w <= 0) {
+        HB_REQUIRE(tol > 0.f && tol < 1.f, HB_ERR_INVALID_ARG, "tol must be in (0,1) when kernel_width <= 0");
+        w = (int)std::ceil(std::log10(10.0 / (double)tol));
+        if (p->sigma < 2.0) {
+            // cufinufft's width rule for low upsampling: ceil(-ln(tol) / (pi sqrt(1 - 1/sigma)))
+            w = (int)std::ceil(-std::log((double)tol) / (M_PI * std::sqrt(1.0 - 1.0 / p->sigma)));
+        }
+        w = std::max(2, std::min(kMaxWidth, w));
+    }
+    HB_REQUIRE(w >= 2 && w <= kMaxWidth, HB_ERR_INVALID_ARG, "kernel width must be in [2, 16]");
+
+    GridGeom& g = p->g;
+    g.dim = dim;
+    g.C = ntransf;
+    for (int ax = 0; ax < 3; ++ax) g.Nm[ax] = 1;
+    for (int i = 0; i < dim; ++i) {
+        HB_REQUIRE(nmodes[i] >= 1 && nmodes[i] <= (1 << 20), HB_ERR_INVALID_ARG, "nmodes out of range");
+        g.Nm[3 - dim + i] = nmodes[i];
+    }
+    // tiles: 8^3 (3-D), 16x32 (2-D), 256 (1-D); wider kernels need tiles >= w-1
+    int Tt[3];
+    if (dim == 3) {
+        const int e = (w <= 9) ? 8 : 16;
+        Tt[0] = Tt[1] = Tt[2] = e;
+    } else if (dim == 2) {
+        Tt[0] = 1;
+        Tt[1] = 16;
+        Tt[2] = 32;
+    } else {
+        Tt[0] = Tt[1] = 1;
+        Tt[2] = 256;
+    }
+    for (int ax = 0; ax < 3; ++ax) {
+        const bool unit = (ax < 3 - dim);
+        g.T[ax] = unit ? 1 : Tt[ax];
+        g.wa[ax] = unit ? 1 : w;
+        g.nf[ax] = unit ? 1 : fine_size(g.Nm[ax], p->sigma, w, g.T[ax]);
+        g.nb[ax] = g.nf[ax] / g.T[ax];
+        g.scale[ax] = (float)((double)g.nf[ax] / (2.0 * M_PI));
+    }
+    p->beta = kb_beta(w, p->sigma);
+    const double fit_err = kb_fit(&p->kb, w, p->beta);
+    if (!(fit_err < 1e-6)) {
+        set_error("kernel polynomial fit failed");
+        return HB_ERR_INVALID_ARG;
+    }
+    p->nbins = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
+
+    // FFT plans and deapodisation factors per axis
+    for (int ax = 0; ax < 3; ++ax) {
+        if (g.nf[ax] > 1) HB_TRY(fftlen_make(&p->fl[ax], g.nf[ax]));
+        std::vector<float> dv((size_t)g.Nm[ax], 1.0f);
+        if (g.nf[ax] > 1) {
+            const int64_t half = g.Nm[ax] / 2;
+            for (int64_t i = 0; i < g.Nm[ax]; ++i) {
+                const double k = (double)(i - half);
+                dv[(size_t)i] = (float)(1.0 / kb_phihat(k / (double)g.nf[ax], w, p->beta));
+            }
+        }
+        HB_TRY(dev_alloc(p, (void**)&p->deapod[ax], sizeof(float) * dv.size(), "deapod"));
+        HB_CUDA(cudaMemcpy(p->deapod[ax], dv.data(), sizeof(float) * dv.size(), cudaMemcpyHostToDevice));
+    }
+    p->X_elems = (size_t)g.nf[0] * g.nf[1] * g.nf[2] * g.C;
+    p->Y_elems = (size_t)g.Nm[0] * g.nf[1] * g.nf[2] * g.C;
+    HB_TRY(dev_alloc(p, (void**)&p->X, sizeof(float2) * p->X_elems, "fine grid"));
+    HB_TRY(dev_alloc(p, (void**)&p->Y, sizeof(float2) * p->Y_elems, "pass buffer"));
+    HB_TRY(dev_alloc(p, (void**)&p->bin_start, sizeof(int) * (p->nbins + 1), "bins"));
+    HB_TRY(dev_alloc(p, (void**)&p->d_err, sizeof(int), "error flag"));
+    return HB_OK;
+}
+
+int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const float* c2, cudaStream_t s) {
+    GridGeom& g = p->g;
+    HB_REQUIRE(M >= 0 && M < (int64_t)0x7fffffff, HB_ERR_INVALID_ARG, "M must be in [0, 2^31)");
+    const float* cu[3] = {c0, c1, c2};
+    const float* ca[3] = {nullptr, nullptr, nullptr};
+    for (int i = 0; i < g.dim; ++i) {
+        HB_REQUIRE(M == 0 || cu[i] != nullptr, HB_ERR_INVALID_ARG, "coordinate array is null");
+        ca[3 - g.dim + i] = cu[i];
+    }
+    if (M > p->M_cap) {
+        for (int ax = 0; ax < 3; ++ax) {
+            if (p->su[ax]) cudaFree(p->su[ax]);
+            p->su[ax] = nullptr;
+        }
+        if (p->perm) cudaFree(p->perm);
+        if (p->inT) cudaFree(p->inT);
+        p->perm = nullptr;
+        p->inT = nullptr;
+        for (int ax = 0; ax < 3; ++ax)
+            if (ca[ax] || g.nf[ax] > 1) HB_TRY(dev_alloc(p, (void**)&p->su[ax], sizeof(float) * M, "sorted coords"));
+        HB_TRY(dev_alloc(p, (void**)&p->perm, sizeof(int) * M, "perm"));
+        if (p->type == 1) HB_TRY(dev_alloc(p, (void**)&p->inT, sizeof(float2) * M * g.C, "sorted input"));
+        p->M_cap = M;
+    }
+    g.M = M;
+    p->pts_set = false;
+
+    // temporaries
+    float* u[3] = {nullptr, nullptr, nullptr};
+    int *binid = nullptr, *rank = nullptr, *count = nullptr, *ecnt = nullptr, *eoff = nullptr;
+    auto cleanup = [&]() {
+        for (int ax = 0; ax < 3; ++ax)
+            if (u[ax]) cudaFree(u[ax]);
+        if (binid) cudaFree(binid);
+        if (rank) cudaFree(rank);
+        if (count) cudaFree(count);
+        if (ecnt) cudaFree(ecnt);
+        if (eoff) cudaFree(eoff);
+    };
+    int st = HB_OK;
+    do {
+        cudaError_t e = cudaSuccess;
+        for (int ax = 0; ax < 3 && e == cudaSuccess; ++ax)
+            if (ca[ax]) e = cudaMalloc(&u[ax], sizeof(float) * std::max<int64_t>(M, 1));
+        if (e == cudaSuccess) e = cudaMalloc(&binid, sizeof(int) * std::max<int64_t>(M, 1));
+        if (e == cudaSuccess) e = cudaMalloc(&rank, sizeof(int) * std::max<int64_t>(M, 1));
+        if (e == cudaSuccess) e = cudaMalloc(&count, sizeof(int) * (p->nbins + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&ecnt, sizeof(int) * (p->nbins + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&eoff, sizeof(int) * (p->nbins + 1));
+        if (e != cudaSuccess) {
+            set_error(std::string("setpts temporaries: ") + cudaGetErrorString(e));
+            st = HB_ERR_ALLOC;
+            break;
+        }
+        if ((e = cudaMemsetAsync(count, 0, sizeof(int) * (p->nbins + 1), s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(p->d_err, 0, sizeof(int), s)) != cudaSuccess) {
+            set_error(std::string("setpts memset: ") + cudaGetErrorString(e));
+            st = HB_ERR_CUDA;
+            break;
+        }
+        if (M > 0) {
+            FoldArgs fa{};
+            for (int ax = 0; ax < 3; ++ax) {
+                fa.c[ax] = ca[ax];
+                fa.u[ax] = u[ax];
+                fa.nf[ax] = g.nf[ax];
+                fa.T[ax] = g.T[ax];
+                fa.nb[ax] = g.nb[ax];
+                fa.scale[ax] = g.scale[ax];
+            }
+            fa.binid = binid;
+            fa.rank = rank;
+            fa.count = count;
+            fa.err = p->d_err;
+            fa.hw = p->kb.hw;
+            fa.M = M;
+            k_fold_bin<<<(unsigned)ceil_div(M, 256), 256, 0, s>>>(fa);
+            if ((st = check_launch("k_fold_bin")) != HB_OK) break;
+        }
+        if ((st = exclusive_scan_int(count, p->bin_start, p->nbins, s)) != HB_OK) break;
+        if (M > 0) {
+            k_scatter_sorted<<<(unsigned)ceil_div(M, 256), 256, 0, s>>>(u[0], u[1], u[2], binid, rank, p->bin_start,
+                                                                       ca[0] ? p->su[0] : nullptr, ca[1] ? p->su[1] : nullptr,
+                                                                       ca[2] ? p->su[2] : nullptr, p->perm, M);
+            if ((st = check_launch("k_scatter_sorted")) != HB_OK) break;
+        }
+        // unit axes: sorted coordinate arrays hold zeros
+        for (int ax = 0; ax < 3; ++ax)
+            if (!ca[ax] && p->su[ax] && M > 0) cudaMemsetAsync(p->su[ax], 0, sizeof(float) * M, s);
+        if (p->type == 1) {
+            TileNbr tn;
+            for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
+            k_tile_extra_count<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins,
+                                                                                kSpreadMaxCand, ecnt);
+            if ((st = check_launch("k_tile_extra_count")) != HB_OK) break;
+            if ((st = exclusive_scan_int(ecnt, eoff, p->nbins, s)) != HB_OK) break;
+            int n_extra = 0, err = 0;
+            if ((e = cudaMemcpyAsync(&n_extra, eoff + p->nbins, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+                set_error(std::string("setpts sync: ") + cudaGetErrorString(e));
+                st = HB_ERR_CUDA;
+                break;
+            }
+            if (err) {
+                set_error("setpts: non-finite coordinate");
+                st = HB_ERR_RANGE;
+                break;
+            }
+            if (n_extra > p->extra_cap) {
+                if (p->extra) cudaFree(p->extra);
+                p->extra = nullptr;
+                if ((st = dev_alloc(p, (void**)&p->extra, sizeof(int2) * n_extra, "spread work list")) != HB_OK) break;
+                p->extra_cap = n_extra;
+            }
+            p->n_extra = n_extra;
+            if (n_extra > 0) {
+                k_tile_extra_fill<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(ecnt, eoff, p->nbins, p->extra);
+                if ((st = check_launch("k_tile_extra_fill")) != HB_OK) break;
+            }
+        }
+        {
+            int err = 0;
+            if ((e = cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+                set_error(std::string("setpts sync: ") + cudaGetErrorString(e));
+                st = HB_ERR_CUDA;
+                break;
+            }
+            if (err) {
+                set_error("setpts: non-finite coordinate");
+                st = HB_ERR_RANGE;
+                break;
+            }
+        }
+    } while (0);
+    cleanup();
+    if (st == HB_OK) p->pts_set = true;
+    return st;
+}
+
+static GridArgs grid_args(const NufftPlan* p) {
+    GridArgs a{};
+    a.g = p->g;
+    for (int ax = 0; ax < 3; ++ax) a.su[ax] = p->su[ax];
+    a.perm = p->perm;
+    a.bin_start = p->bin_start;
+    a.inT = p->inT;
+    a.grid = p->X;
+    a.extra = p->extra;
+    a.maxp = kSpreadMaxCand;
+    a.kb = p->kb;
+    return a;
+}
+
+template <int CC>
+static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
+    const GridGeom& g = p->g;
+    const int cells = g.T[0] * g.T[1] * g.T[2];
+    const size_t smem = sizeof(float) * ((size_t)2 * cells * CC + kCoefFloats + (size_t)kGridWarps * (32 / CC) * kSlotFloats);
+    HB_CUDA(cudaFuncSetAttribute(k_spread<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    {
+        TimedSection ts("spread", s);
+        k_spread<CC><<<(unsigned)p->nbins, kGridThreads, smem, s>>>(a, 0);
+        HB_TRY(check_launch("k_spread"));
+    }
+    if (p->n_extra > 0) {
+        TimedSection ts("spread_dense", s);
+        k_spread<CC><<<(unsigned)p->n_extra, kGridThreads, smem, s>>>(a, 1);
+        HB_TRY(check_launch("k_spread(extra)"));
+    }
+    return HB_OK;
+}
+
+template <int CC>
+static int launch_interp_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
+    const int64_t per_block = (int64_t)kGridWarps * (32 / CC);
+    int64_t blocks = ceil_div(std::max<int64_t>(p->g.M, 1), per_block);
+    blocks = std::min<int64_t>(blocks, (int64_t)kNumSMs * 64);
+    const size_t smem = sizeof(float) * (kCoefFloats + (size_t)kGridWarps * (32 / CC) * kSlotFloats);
+    HB_CUDA(cudaFuncSetAttribute(k_interp<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TimedSection ts("interp", s);
+    k_interp<CC><<<(unsigned)blocks, kGridThreads, smem, s>>>(a);
+    return check_launch("k_interp");
+}
+
+static int dispatch_cc(int cc, const NufftPlan* p, const GridArgs& a, cudaStream_t s, bool spread) {
+    switch (cc) {
+        case 1: return spread ? launch_spread_cc<1>(p, a, s) : launch_interp_cc<1>(p, a, s);
+        case 2: return spread ? launch_spread_cc<2>(p, a, s) : launch_interp_cc<2>(p, a, s);
+        case 4: return spread ? launch_spread_cc<4>(p, a, s) : launch_interp_cc<4>(p, a, s);
+        case 8: return spread ? launch_spread_cc<8>(p, a, s) : launch_interp_cc<8>(p, a, s);
+        case 16: return spread ? launch_spread_cc<16>(p, a, s) : launch_interp_cc<16>(p, a, s);
+        default: return spread ? launch_spread_cc<32>(p, a, s) : launch_interp_cc<32>(p, a, s);
+    }
+}
+
+int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
+    HB_REQUIRE(p->pts_set, HB_ERR_STATE, "execute called before setpts");
+    const GridGeom& g = p->g;
+    // the nonuniform side may be empty (M == 0), the mode side never is
+    const bool in_ok = in != nullptr || (p->type == 1 && g.M == 0);
+    const bool out_ok = out != nullptr || (p->type == 2 && g.M == 0);
+    HB_REQUIRE(in_ok && out_ok, HB_ERR_INVALID_ARG, "null data pointer");
+    const int C = g.C;
+    const int64_t M = g.M;
+    const int64_t nm = g.Nm[0] * g.Nm[1] * g.Nm[2];
+    const bool inv = p->sign > 0;
+    const int64_t h0 = g.Nm[0] / 2, h1 = g.Nm[1] / 2, h2 = g.Nm[2] / 2;
+
+    if (p->type == 1) {
+        if (M > 0) {
+            TimedSection ts("permute_in", s);
+            k_permute_in<<<(unsigned)ceil_div(M * C, 256), 256, 0, s>>>(in, p->perm, p->inT, M, C);
+            HB_TRY(check_launch("k_permute_in"));
+        }
+        GridArgs a = grid_args(p);
+        HB_TRY(dispatch_cc(spread_cc(g), p, a, s, true));
+        float2* cur = p->X;
+        float2* other = p->Y;
+        // axis 0: [nf0][nf1*nf2*C] -> [Nm0][...]
+        if (g.nf[0] > 1) {
+            PassCfg c;
+            const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
+            pass_setup(&c, p->fl[0], 1, E, g.nf[0], 0, (int)g.Nm[0], (int)-h0, inv);
+            OpStrided op{cur, other, 0, E, 0, E, 1.0f};
+            HB_TRY(launch_pass(op, c, 0, s, "type1 axis0"));
+            std::swap(cur, other);
+        }
+        // axis 1: [Nm0][nf1][nf2*C] -> [Nm0][Nm1][nf2*C]
+        if (g.nf[1] > 1) {
+            PassCfg c;
+            const int64_t E = (int64_t)g.nf[2] * C;
+            pass_setup(&c, p->fl[1], g.Nm[0], E, g.nf[1], 0, (int)g.Nm[1], (int)-h1, inv);
+            OpStrided op{cur, other, (int64_t)g.nf[1] * E, E, g.Nm[1] * E, E, 1.0f};
+            HB_TRY(launch_pass(op, c, 0, s, "type1 axis1"));
+            std::swap(cur, other);
+        }
+        // axis 2 -> caller's modes with deapodisation
+        {
+            PassCfg c;
+            pass_setup(&c, p->fl[2], g.Nm[0] * g.Nm[1], C, g.nf[2], 0, (int)g.Nm[2], (int)-h2, inv);
+            OpModesOut op{cur, out, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm,
+                          (int64_t)g.nf[2] * C, C};
+            HB_TRY(launch_pass(op, c, 0, s, "type1 axis2"));
+        }
+        return HB_OK;
+    }
+
+    // type 2: passes x, y, z then interpolate from X
+    const int npass = 1 + (g.nf[1] > 1) + (g.nf[0] > 1);
+    float2* cur = (npass % 2 == 1) ? p->X : p->Y;
+    float2* other = (cur == p->X) ? p->Y : p->X;
+    {
+        PassCfg c;
+        pass_setup(&c, p->fl[2], g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv);
+        OpModesIn op{in, cur, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm, (int64_t)g.nf[2] * C, C};
+        HB_TRY(launch_pass(op, c, 0, s, "type2 axis2"));
+    }
+    if (g.nf[1] > 1) {
+        PassCfg c;
+        const int64_t E = (int64_t)g.nf[2] * C;
+        pass_setup(&c, p->fl[1], g.Nm[0], E, (int)g.Nm[1], (int)-h1, g.nf[1], 0, inv);
+        OpStrided op{cur, other, g.Nm[1] * E, E, (int64_t)g.nf[1] * E, E, 1.0f};
+        HB_TRY(launch_pass(op, c, 0, s, "type2 axis1"));
+        std::swap(cur, other);
+    }
+    if (g.nf[0] > 1) {
+        PassCfg c;
+        const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
+        pass_setup(&c, p->fl[0], 1, E, (int)g.Nm[0], (int)-h0, g.nf[0], 0, inv);
+        OpStrided op{cur, other, 0, E, 0, E, 1.0f};
+        HB_TRY(launch_pass(op, c, 0, s, "type2 axis0"));
+        std::swap(cur, other);
+    }
+    if (M > 0) {
+        GridArgs a = grid_args(p);
+        a.grid = cur;
+        a.out = out;
+        HB_TRY(dispatch_cc(spread_cc(g), p, a, s, false));
+    }
+    return HB_OK;
+}
+
+void plan_free(NufftPlan* p) {
+    for (int ax = 0; ax < 3; ++ax) {
+        fftlen_free(&p->fl[ax]);
+        if (p->deapod[ax]) cudaFree(p->deapod[ax]);
+        if (p->su[ax]) cudaFree(p->su[ax]);
+        p->deapod[ax] = nullptr;
+        p->su[ax] = nullptr;
+    }
+    if (p->X) cudaFree(p->X);
+    if (p->Y) cudaFree(p->Y);
+    if (p->perm) cudaFree(p->perm);
+    if (p->inT) cudaFree(p->inT);
+    if (p->bin_start) cudaFree(p->bin_start);
+    if (p->extra) cudaFree(p->extra);
+    if (p->d_err) cudaFree(p->d_err);
+    p->X = p->Y = nullptr;
+    p->perm = nullptr;
+    p->inT = nullptr;
+    p->bin_start = nullptr;
+    p->extra = nullptr;
+    p->d_err = nullptr;
+}
+
+}  // namespace hb

@@ -1,0 +1,72 @@
+// NUFFT plan internals (type 1 / type 2, 1-3 dimensions, complex64, Kaiser-Bessel).
+//
+// Internally every problem is 3-D with unit leading axes: a 2-D plan of [N1, N2] is
+// [1, N1, N2]. Axis 0 is the slowest. A unit axis has one mode, one fine cell, tap width 1.
+//
+// Device data layout:
+//   fine grid     X[nf0][nf1][nf2][C]   (transforms interleaved: one cell holds all C values)
+//   pass buffer   Y[Nm0][nf1][nf2][C]   (the grid after/before the axis-0 transform)
+//   sorted points su_a[M] (fine coordinates in [0, nf_a)), perm[M] (sorted -> caller index)
+//   bins          bin_start[nbins+1]   (tiles of T0 x T1 x T2 cells; bins == tiles)
+#pragma once
+
+#include <stdint.h>
+
+#include "fft.cuh"
+#include "kbkernel.cuh"
+
+namespace hb {
+
+struct GridGeom {
+    int dim;          // caller's dimensionality (1..3)
+    int C;            // transforms (ntransf)
+    int64_t Nm[3];    // modes per axis
+    int nf[3];        // fine cells per axis
+    int wa[3];        // taps per axis (1 on unit axes)
+    int T[3];         // tile edge per axis
+    int nb[3];        // tiles (bins) per axis
+    float scale[3];   // nf / (2 pi), float32
+    int64_t M;        // points
+};
+
+struct NufftPlan {
+    int type = 1;
+    int sign = 1;
+    int method = HB_METHOD_DEFAULT;
+    double sigma = 2.0;
+    double beta = 0.0;
+    GridGeom g{};
+    KbPoly kb{};
+    FftLen fl[3];
+    float* deapod[3] = {nullptr, nullptr, nullptr};
+    float2* X = nullptr;
+    float2* Y = nullptr;
+    size_t X_elems = 0, Y_elems = 0;
+    // points
+    int64_t M_cap = 0;
+    float* su[3] = {nullptr, nullptr, nullptr};
+    int* perm = nullptr;
+    float2* inT = nullptr;  // type 1: [M][C] sorted copy of the input
+    int* bin_start = nullptr;
+    int64_t nbins = 0;
+    int2* extra = nullptr;  // spread subproblems beyond the first chunk of each tile
+    int64_t n_extra = 0;
+    int64_t extra_cap = 0;
+    int* d_err = nullptr;
+    bool pts_set = false;
+    size_t device_bytes = 0;
+};
+
+// Candidates (points of the up to 8 bins that can reach a tile) per spread subproblem.
+constexpr int kSpreadMaxCand = 1024;
+
+int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, int ntransf, float tol,
+              int width, double upsampfac, int method);
+int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const float* c2, cudaStream_t s);
+int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s);
+void plan_free(NufftPlan* p);
+
+// Pieces reused by the Toeplitz kernel builder.
+int exclusive_scan_int(const int* in, int* out, int64_t n, cudaStream_t s);
+
+}  // namespace hb

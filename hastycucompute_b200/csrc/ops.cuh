@@ -1,0 +1,38 @@
+// Pass operators shared by the NUFFT and Toeplitz paths (see fft.cuh for the Op contract).
+#pragma once
+
+#include "fft.cuh"
+
+namespace hb {
+
+#ifdef __CUDACC__
+
+// Plain strided transform: element (a, l, e) at base + a*s_a + l*s_l + e on both sides.
+struct OpStrided {
+    static constexpr bool kLoadLFast = false;
+    static constexpr bool kFusedK = false;
+    static constexpr bool kChunkLoop = false;
+    const float2* src;
+    float2* dst;
+    int64_t s_a, s_l;
+    int64_t d_a, d_l;
+    float scale;
+    __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
+        return src[a * s_a + (int64_t)l * s_l + e];
+    }
+    __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
+                                                float2*) const {
+        const float sc = scale;
+        float2* d = dst;
+        const int64_t da = d_a, dl = d_l;
+        for_each_output<false>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) {
+            d[a * da + (int64_t)o * dl + e] = cscale(v, sc);
+        });
+    }
+    __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
+};
+
+#endif
+
+}  // namespace hb

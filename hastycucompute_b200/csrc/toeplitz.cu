@@ -1,0 +1,486 @@
+// Toeplitz-embedded normal operator on B200: kernel construction, kernel re-layout, the fused
+// 2x-padded convolution with the reference's multiply flags, and the SENSE normal operator.
+//
+// The convolution never materialises a (2N)^d grid per batch. With B batches interleaved in
+// one buffer ([..][B], B fastest), a 3-D apply is five pruned passes:
+//   P1 axis 2: load in[b] * mults (N2 samples) -> FFT 2N2            -> W1[N0][N1][2N2][B]
+//   P2 axis 1: N1 samples -> FFT 2N1                                 -> W2[N0][2N1][2N2][B]
+//   P3 axis 0: N0 samples -> FFT 2N0, * K, IFFT 2N0, keep [N0-1,2N0-1) -> W2 (in place)
+//   P4 axis 1: IFFT 2N1, keep [N1-1, 2N1-1)                          -> W1[N0][N1][2N2][B]
+//   P5 axis 2: IFFT 2N2, keep [N2-1, 2N2-1), * output mults (and for SENSE: sum over b of
+//              conj(S_b) * v inside the CTA)                          -> out
+// A 2-D apply is P1, the fused pass along axis 1, and P5.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "nufft.cuh"
+#include "ops.cuh"
+
+namespace hb {
+
+struct ToepGeom {
+    int dim;
+    int64_t N[3];  // internal 3-D (N0 == 1 in 2-D)
+    int L[3];      // 2N on non-unit axes, 1 on unit axes
+    int64_t n;     // N0*N1*N2
+    int64_t B;
+};
+
+static int toep_geom(ToepGeom* t, int dim, const int64_t* shape, int64_t B) {
+    HB_REQUIRE(dim == 2 || dim == 3, HB_ERR_INVALID_ARG, "Toeplitz operator supports dim 2 and 3");
+    HB_REQUIRE(shape != nullptr, HB_ERR_INVALID_ARG, "shape is null");
+    HB_REQUIRE(B >= 1, HB_ERR_INVALID_ARG, "batch count must be >= 1");
+    t->dim = dim;
+    t->B = B;
+    t->n = 1;
+    for (int ax = 0; ax < 3; ++ax) {
+        t->N[ax] = 1;
+        t->L[ax] = 1;
+    }
+    for (int i = 0; i < dim; ++i) {
+        const int64_t v = shape[i];
+        HB_REQUIRE(v > 1 && v <= (1 << 15), HB_ERR_INVALID_ARG, "image dimensions must be in (1, 32768]");
+        t->N[3 - dim + i] = v;
+        t->L[3 - dim + i] = (int)(2 * v);
+        t->n *= v;
+    }
+    for (int ax = 3 - dim; ax < 3; ++ax) {
+        int r = t->L[ax];
+        for (int p : {2, 3, 5, 7})
+            while (r % p == 0) r /= p;
+        HB_REQUIRE(r == 1, HB_ERR_INVALID_ARG, "2N must be 2,3,5,7-smooth on every axis");
+    }
+    return HB_OK;
+}
+
+static size_t toep_ws_elems(const ToepGeom& t) {
+    size_t w1 = (size_t)t.N[0] * t.N[1] * t.L[2] * t.B;
+    size_t w2 = t.dim == 3 ? (size_t)t.N[0] * t.L[1] * t.L[2] * t.B : 0;
+    return w1 + w2;
+}
+
+// Per-thread cache of FFT length plans (twiddle tables) keyed by length and device. The first
+// use of a length uploads its table with synchronous copies, so it must happen outside a stream
+// capture; later uses only read the cache.
+struct LenCache {
+    int dev;
+    FftLen f;
+};
+static thread_local std::vector<LenCache> g_len_cache;
+
+static int get_len(int L, FftLen* out) {
+    int dev = 0;
+    HB_CUDA(cudaGetDevice(&dev));
+    for (const auto& c : g_len_cache)
+        if (c.dev == dev && c.f.L == L) {
+            *out = c.f;
+            return HB_OK;
+        }
+    LenCache c;
+    c.dev = dev;
+    HB_TRY(fftlen_make(&c.f, L));
+    g_len_cache.push_back(c);
+    *out = c.f;
+    return HB_OK;
+}
+
+// ---- ops -------------------------------------------------------------------------------------
+#ifdef __CUDACC__
+
+struct OpToepIn {
+    static constexpr bool kLoadLFast = true;
+    static constexpr bool kFusedK = false;
+    static constexpr bool kChunkLoop = false;
+    const float2* in;
+    const float2* m1;
+    const float2* m2;
+    int in_m1, in_m2;
+    float2* dst;
+    int64_t N2, n, d_a, d_l;
+    __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
+        const int64_t idx = a * N2 + l;
+        float2 v = in[e * n + idx];
+        if (m1) v = mult_typed(v, m1[idx], in_m1);
+        if (m2) v = mult_typed(v, m2[idx], in_m2);
+        return v;
+    }
+    __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
+                                                float2*) const {
+        float2* d = dst;
+        const int64_t da = d_a, dl = d_l;
+        for_each_output<false>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) { d[a * da + (int64_t)o * dl + e] = v; });
+    }
+    __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
+};
+
+// In-place fused pass: FFT, * Kt[col][pos], IFFT, crop. buf[l][e] with row stride E.
+struct OpToepMid {
+    static constexpr bool kLoadLFast = false;
+    static constexpr bool kFusedK = true;
+    static constexpr bool kChunkLoop = false;
+    float2* buf;
+    const float2* kt;
+    int64_t E, B;
+    int Lk;
+    __device__ __forceinline__ float2 load(int64_t, int l, int64_t e) const { return buf[(int64_t)l * E + e]; }
+    __device__ __forceinline__ float2 kval(int64_t, int pos, int64_t e) const { return kt[(e / B) * Lk + pos]; }
+    __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
+                                                float2*) const {
+        float2* d = buf;
+        const int64_t EE = E;
+        for_each_output<false>(res, c, a0, e0, [&](int64_t, int o, int64_t e, float2 v) { d[(int64_t)o * EE + e] = v; });
+    }
+    __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
+};
+
+struct OpToepOutFlat {
+    static constexpr bool kLoadLFast = false;
+    static constexpr bool kFusedK = false;
+    static constexpr bool kChunkLoop = false;
+    const float2* src;  // [rows][L2][B]
+    int64_t s_a, s_l;
+    const float2* in;
+    const float2* m1;
+    const float2* m2;
+    int io_mult, out_m1, out_m2, accumulate;
+    float2* out;
+    int64_t N2, n;
+    __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
+    __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
+                                                float2*) const {
+        for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) {
+            const int64_t idx = a * N2 + o;
+            if (m1) v = mult_typed(v, m1[idx], out_m1);
+            if (m2) v = mult_typed(v, m2[idx], out_m2);
+            if (io_mult) v = mult_typed(v, in[e * n + idx], io_mult);
+            float2* dst = out + e * n + idx;
+            if (accumulate) v = cadd(v, *dst);
+            *dst = v;
+        });
+    }
+    __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
+};
+
+// Last pass of the SENSE normal operator: out[a][o] = sum_b conj(S_b[a][o]) * v_b[a][o]. The CTA
+// walks every batch chunk of its rows and keeps the running sum in shared memory (extra).
+struct OpToepOutSense {
+    static constexpr bool kLoadLFast = false;
+    static constexpr bool kFusedK = false;
+    static constexpr bool kChunkLoop = true;
+    const float2* src;
+    int64_t s_a, s_l;
+    const float2* smaps;
+    float2* out;
+    int64_t N2, n;
+    __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
+    __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int Ab, int Eb,
+                                                float2* acc) const {
+        const int tot = Ab * c.Lout;
+        for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+            const int o = idx % c.Lout, al = idx / c.Lout;
+            const int64_t a = a0 + al;
+            if (a >= c.A) continue;
+            int pos = (o + c.out_shift) % c.L;
+            if (pos < 0) pos += c.L;
+            const int64_t idx_img = a * N2 + o;
+            float2 sum = (e0 == 0) ? make_float2(0.f, 0.f) : acc[idx];
+            for (int el = 0; el < Eb; ++el) {
+                const int64_t e = e0 + el;
+                if (e >= c.E) break;
+                const float2 v = res[pos * c.Wp + al * Eb + el];
+                const float2 sv = smaps[e * n + idx_img];
+                sum = cadd(sum, cmulc(v, sv));
+            }
+            acc[idx] = sum;
+        }
+    }
+    __device__ __forceinline__ void finish(const PassCfg& c, int64_t a0, float2* acc) const {
+        const int tot = c.A_blk * c.Lout;
+        for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+            const int o = idx % c.Lout, al = idx / c.Lout;
+            const int64_t a = a0 + al;
+            if (a >= c.A) continue;
+            out[a * N2 + o] = acc[idx];
+        }
+    }
+};
+
+// Kt[(c)*L + z] = K[z][c] * scale : transpose [R][Ccols] -> [Ccols][R]
+__global__ void k_transpose_scale(const float2* __restrict__ in, float2* __restrict__ out, int64_t R, int64_t Cc, float scale) {
+    __shared__ float2 tile[32][33];
+    const int64_t c0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t r = r0 + j, c = c0 + threadIdx.x;
+        if (r < R && c < Cc) tile[j][threadIdx.x] = in[r * Cc + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t c = c0 + j, r = r0 + threadIdx.x;
+        if (r < R && c < Cc) out[c * R + r] = cscale(tile[threadIdx.x][j], scale);
+    }
+}
+
+#endif
+
+// ---- the convolution --------------------------------------------------------------------------
+struct ToepArgs {
+    const float2* in;
+    float2* out;
+    const float2* kt;
+    const float2* m1;
+    const float2* m2;
+    int io_mult, in_m1, out_m1, in_m2, out_m2, accumulate;
+    bool sense;
+};
+
+static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream_t s) {
+    const int64_t B = t.B;
+    const int64_t N0 = t.N[0], N1 = t.N[1], N2 = t.N[2];
+    const int L0 = t.L[0], L1 = t.L[1], L2 = t.L[2];
+    float2* W1 = ws;                                   // [N0][N1][L2][B]
+    float2* W2 = ws + (size_t)N0 * N1 * L2 * B;        // [N0][L1][L2][B] (3-D only)
+    FftLen f0, f1, f2;
+    HB_TRY(get_len(L2, &f2));
+    HB_TRY(get_len(L1, &f1));
+    if (t.dim == 3) HB_TRY(get_len(L0, &f0));
+
+    // P1: axis 2, pad N2 -> L2, forward
+    {
+        PassCfg c;
+        pass_setup(&c, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0);
+        OpToepIn op{a.in, a.m1, a.m2, a.in_m1, a.in_m2, W1, N2, t.n, (int64_t)L2 * B, B};
+        HB_TRY(launch_pass(op, c, 0, s, "toeplitz P1"));
+    }
+    const int64_t E2 = (int64_t)L2 * B;
+    if (t.dim == 3) {
+        // P2: axis 1, pad N1 -> L1, forward
+        {
+            PassCfg c;
+            pass_setup(&c, f1, N0, E2, (int)N1, 0, L1, 0, 0);
+            OpStrided op{W1, W2, N1 * E2, E2, (int64_t)L1 * E2, E2, 1.0f};
+            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P2"));
+        }
+        // P3: axis 0 fused, in place on W2
+        {
+            PassCfg c;
+            const int64_t E = (int64_t)L1 * E2;
+            pass_setup(&c, f0, 1, E, (int)N0, 0, (int)N0, (int)(N0 - 1), 0);
+            OpToepMid op{W2, a.kt, E, B, L0};
+            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P3"));
+        }
+        // P4: axis 1 inverse, crop -> W1
+        {
+            PassCfg c;
+            pass_setup(&c, f1, N0, E2, L1, 0, (int)N1, (int)(N1 - 1), 1);
+            OpStrided op{W2, W1, (int64_t)L1 * E2, E2, N1 * E2, E2, 1.0f};
+            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P4"));
+        }
+    } else {
+        // fused pass along axis 1, in place on W1 ([1][N1][L2][B])
+        PassCfg c;
+        pass_setup(&c, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0);
+        OpToepMid op{W1, a.kt, E2, B, L1};
+        HB_TRY(launch_pass(op, c, 0, s, "toeplitz P3"));
+    }
+    // P5: axis 2 inverse, crop, output ops
+    {
+        PassCfg c;
+        pass_setup(&c, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1);
+        if (a.sense) {
+            OpToepOutSense op{W1, (int64_t)L2 * B, B, a.in, a.out, N2, t.n};
+            HB_TRY(launch_pass(op, c, sizeof(float2) * (size_t)c.A_blk * c.Lout, s, "toeplitz P5 sense"));
+        } else {
+            OpToepOutFlat op{W1, (int64_t)L2 * B, B, a.in, a.m1, a.m2, a.io_mult, a.out_m1, a.out_m2, a.accumulate,
+                             a.out, N2, t.n};
+            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P5"));
+        }
+    }
+    return HB_OK;
+}
+
+static bool valid_mult(int m) { return m == HB_MULT_NONE || m == HB_MULT_MULT || m == HB_MULT_MULT_CONJ; }
+
+struct WsGuard {
+    float2* ptr = nullptr;
+    bool owned = false;
+    cudaStream_t s = nullptr;
+    ~WsGuard() {
+        if (owned && ptr) cudaFreeAsync(ptr, s);
+    }
+};
+
+static int get_workspace(const ToepGeom& t, void* ws, size_t ws_bytes, cudaStream_t s, WsGuard* g) {
+    const size_t need = toep_ws_elems(t) * sizeof(float2);
+    if (ws) {
+        if (ws_bytes < need) {
+            set_error("workspace too small: need " + std::to_string(need) + " bytes, got " + std::to_string(ws_bytes));
+            return HB_ERR_WORKSPACE;
+        }
+        g->ptr = (float2*)ws;
+        return HB_OK;
+    }
+    g->s = s;
+    cudaError_t e = cudaMallocAsync((void**)&g->ptr, need, s);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaMallocAsync(workspace) failed: ") + cudaGetErrorString(e));
+        g->ptr = nullptr;
+        return HB_ERR_ALLOC;
+    }
+    g->owned = true;
+    return HB_OK;
+}
+
+int toeplitz_workspace_size(int dim, const int64_t* shape, int64_t nbatch, size_t* bytes) {
+    ToepGeom t;
+    HB_TRY(toep_geom(&t, dim, shape, nbatch));
+    HB_REQUIRE(bytes != nullptr, HB_ERR_INVALID_ARG, "bytes is null");
+    *bytes = toep_ws_elems(t) * sizeof(float2);
+    return HB_OK;
+}
+
+int toeplitz_multiplication(int dim, const int64_t* shape, int64_t nbatch, const void* input, void* output,
+                            const void* kernel, void* workspace, size_t workspace_bytes, const void* mult1,
+                            const void* mult2, int io_mult, int in_m1, int out_m1, int in_m2, int out_m2, int accumulate,
+                            cudaStream_t s) {
+    ToepGeom t;
+    HB_TRY(toep_geom(&t, dim, shape, nbatch));
+    HB_REQUIRE(input && output && kernel, HB_ERR_INVALID_ARG, "input, output and kernel must be non-null");
+    HB_REQUIRE(valid_mult(io_mult), HB_ERR_INVALID_ARG, "Invalid input_output_mult_type");
+    HB_REQUIRE(valid_mult(in_m1), HB_ERR_INVALID_ARG, "Invalid input_mult_type");
+    HB_REQUIRE(valid_mult(out_m1), HB_ERR_INVALID_ARG, "Invalid output_mult_type");
+    HB_REQUIRE(valid_mult(in_m2), HB_ERR_INVALID_ARG, "Invalid input_mult2_type");
+    HB_REQUIRE(valid_mult(out_m2), HB_ERR_INVALID_ARG, "Invalid output_mult2_type");
+    HB_REQUIRE(accumulate == HB_ACC_NONE || accumulate == HB_ACC_ACCUMULATE, HB_ERR_INVALID_ARG, "Invalid accumulate_type");
+    WsGuard g;
+    HB_TRY(get_workspace(t, workspace, workspace_bytes, s, &g));
+    ToepArgs a{};
+    a.in = (const float2*)input;
+    a.out = (float2*)output;
+    a.kt = (const float2*)kernel;
+    a.m1 = (const float2*)mult1;
+    a.m2 = (const float2*)mult2;
+    a.io_mult = io_mult;
+    a.in_m1 = in_m1;
+    a.out_m1 = out_m1;
+    a.in_m2 = in_m2;
+    a.out_m2 = out_m2;
+    a.accumulate = accumulate;
+    a.sense = false;
+    return toep_run(t, a, g.ptr, s);
+}
+
+int sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps, const void* kernel,
+                 void* out, void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    ToepGeom t;
+    HB_TRY(toep_geom(&t, dim, shape, ncoils));
+    HB_REQUIRE(x && smaps && kernel && out, HB_ERR_INVALID_ARG, "x, smaps, kernel and out must be non-null");
+    HB_REQUIRE(out != x, HB_ERR_INVALID_ARG, "out must not alias x");
+    WsGuard g;
+    HB_TRY(get_workspace(t, workspace, workspace_bytes, s, &g));
+    ToepArgs a{};
+    a.in = (const float2*)smaps;
+    a.out = (float2*)out;
+    a.kt = (const float2*)kernel;
+    a.m1 = (const float2*)x;
+    a.m2 = nullptr;
+    a.in_m1 = HB_MULT_MULT;
+    a.in_m2 = HB_MULT_NONE;
+    a.sense = true;
+    return toep_run(t, a, g.ptr, s);
+}
+
+int transform_toeplitz_kernel(int dim, const int64_t* kshape, const void* kin, void* kout, cudaStream_t s) {
+    HB_REQUIRE(dim == 2 || dim == 3, HB_ERR_INVALID_ARG, "Toeplitz kernel must be 2-D or 3-D");
+    HB_REQUIRE(kshape && kin && kout, HB_ERR_INVALID_ARG, "null argument");
+    HB_REQUIRE(kin != kout, HB_ERR_INVALID_ARG, "kernel_in and kernel_out must not alias");
+    int64_t R = kshape[0], Cc = 1, tot = 1;
+    for (int i = 0; i < dim; ++i) {
+        HB_REQUIRE(kshape[i] >= 2 && kshape[i] % 2 == 0, HB_ERR_SHAPE, "kernel dimensions must be even (2N)");
+        tot *= kshape[i];
+        if (i > 0) Cc *= kshape[i];
+    }
+    const float scale = (float)(1.0 / (double)tot);
+    dim3 grid((unsigned)ceil_div(Cc, 32), (unsigned)ceil_div(R, 32));
+    k_transpose_scale<<<grid, dim3(32, 8), 0, s>>>((const float2*)kin, (float2*)kout, R, Cc, scale);
+    return check_launch("transform_toeplitz_kernel");
+}
+
+int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, const float* c1, const float* c2,
+                    const void* nudata, void* kout, int width, cudaStream_t s) {
+    HB_REQUIRE(dim >= 2 && dim <= 3, HB_ERR_INVALID_ARG, "Toeplitz kernel must be 2-D or 3-D");
+    HB_REQUIRE(kshape && nudata && kout, HB_ERR_INVALID_ARG, "null argument");
+    int64_t nm[3], L[3] = {1, 1, 1}, Nimg = 1;
+    for (int i = 0; i < dim; ++i) {
+        HB_REQUIRE(kshape[i] >= 4 && kshape[i] % 2 == 0, HB_ERR_SHAPE, "kernel dimensions must be even (2N)");
+        nm[i] = kshape[i] - 1;
+        L[3 - dim + i] = kshape[i];
+        Nimg *= kshape[i] / 2;
+    }
+    NufftPlan plan;
+    int st = plan_make(&plan, 1, dim, nm, 1, 1, 1e-5f, width, 2.0, HB_METHOD_DEFAULT);
+    float2 *red = nullptr, *b1 = nullptr, *b2 = nullptr;
+    auto cleanup = [&]() {
+        plan_free(&plan);
+        if (red) cudaFree(red);
+        if (b1) cudaFree(b1);
+        if (b2) cudaFree(b2);
+    };
+    if (st != HB_OK) {
+        cleanup();
+        return st;
+    }
+    const int64_t r0 = L[0] > 1 ? L[0] - 1 : 1, r1 = L[1] - 1, r2 = L[2] - 1;
+    const size_t nred = (size_t)r0 * r1 * r2;
+    cudaError_t e = cudaMalloc(&red, sizeof(float2) * nred);
+    if (e == cudaSuccess) e = cudaMalloc(&b1, sizeof(float2) * (size_t)r0 * r1 * L[2]);
+    if (e == cudaSuccess) e = cudaMalloc(&b2, sizeof(float2) * (size_t)r0 * L[1] * L[2]);
+    if (e != cudaSuccess) {
+        cleanup();
+        set_error(std::string("toeplitz_kernel temporaries: ") + cudaGetErrorString(e));
+        return HB_ERR_ALLOC;
+    }
+    do {
+        if ((st = plan_setpts(&plan, M, c0, c1, c2, s)) != HB_OK) break;
+        if ((st = plan_execute(&plan, (const float2*)nudata, red, s)) != HB_OK) break;
+        FftLen f0, f1, f2;
+        if ((st = get_len((int)L[2], &f2)) != HB_OK) break;
+        if ((st = get_len((int)L[1], &f1)) != HB_OK) break;
+        if (dim == 3 && (st = get_len((int)L[0], &f0)) != HB_OK) break;
+        const float scale = (float)(1.0 / (double)Nimg);
+        float2* K = (float2*)kout;
+        // axis 2: [r0*r1][r2] -> b1 [r0*r1][L2]
+        {
+            PassCfg c;
+            pass_setup(&c, f2, r0 * r1, 1, (int)r2, 0, (int)L[2], 0, 0);
+            OpStrided op{red, b1, r2, 1, L[2], 1, 1.0f};
+            if ((st = launch_pass(op, c, 0, s, "toeplitz_kernel axis2")) != HB_OK) break;
+        }
+        // axis 1: [r0][r1][L2] -> [r0][L1][L2]
+        {
+            PassCfg c;
+            pass_setup(&c, f1, r0, L[2], (int)r1, 0, (int)L[1], 0, 0);
+            float2* dst = dim == 3 ? b2 : K;
+            OpStrided op{b1, dst, r1 * L[2], L[2], L[1] * L[2], L[2], dim == 3 ? 1.0f : scale};
+            if ((st = launch_pass(op, c, 0, s, "toeplitz_kernel axis1")) != HB_OK) break;
+        }
+        if (dim == 3) {
+            PassCfg c;
+            const int64_t E = L[1] * L[2];
+            pass_setup(&c, f0, 1, E, (int)r0, 0, (int)L[0], 0, 0);
+            OpStrided op{b2, K, 0, E, 0, E, scale};
+            if ((st = launch_pass(op, c, 0, s, "toeplitz_kernel axis0")) != HB_OK) break;
+        }
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+            set_error(std::string("toeplitz_kernel sync: ") + cudaGetErrorString(e));
+            st = HB_ERR_CUDA;
+        }
+    } while (0);
+    cleanup();
+    return st;
+}
+
+}  // namespace hb

@@ -1,0 +1,189 @@
+/*
+ * hasty_b200.h -- C ABI of libhasty_b200.so, the B200 (sm_100a) implementation of the
+ * HastyCuCompute MRI reconstruction hot path:
+ *
+ *   - non-uniform FFT type 1 (adjoint gridding) and type 2 (forward interpolation),
+ *     1-3 dimensions, complex64 data, float32 coordinates in radians;
+ *   - the Toeplitz-embedded normal operator (2x zero pad, FFT, pointwise kernel, crop),
+ *     its kernel construction, and the SENSE coil expand / reduce around it;
+ *   - the conjugate-gradient vector steps that drive the normal operator.
+ *
+ * Conventions (all shared with the reference C++ library):
+ *   - arrays are C-order; an image of shape [N0, N1, N2] has N2 fastest;
+ *   - coordinate array coordI pairs with image dimension I (the reference hands
+ *     coords[DIM-1] to cufinufft as "x", cpp/corelib/lib/fft/nufft.cppm:191-199);
+ *   - mode index i of a dimension of size N holds frequency k = i - floor(N/2)
+ *     (cufinufft default mode order);
+ *   - type 1:  f[k]  = sum_j c_j exp(+i*sign1 k.x_j), default sign +1;
+ *     type 2:  c_j   = sum_k f[k] exp(+i*sign2 k.x_j), default sign -1
+ *     (cpp/corelib/lib/fft/nufft.cppm:50-55);
+ *   - every device pointer is caller-owned unless a function says otherwise;
+ *   - every launch goes on the caller's stream (`stream` is a cudaStream_t, NULL means the
+ *     legacy default stream); nothing synchronises the device except where stated.
+ *
+ * Errors: every function returns an int status (HB_OK == 0). On failure the message is
+ * kept per thread and returned by hb_last_error(). Nothing throws across this boundary.
+ */
+#ifndef HASTY_B200_H
+#define HASTY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define HB_OK               0
+#define HB_ERR_INVALID_ARG  1  /* bad enum value, null pointer, bad sizes              */
+#define HB_ERR_SHAPE        2  /* shapes that do not agree (kernel vs image, ...)       */
+#define HB_ERR_CUDA         3  /* a CUDA runtime call failed                             */
+#define HB_ERR_ALLOC        4  /* device allocation failed                               */
+#define HB_ERR_STATE        5  /* call order violated (execute before setpts, ...)      */
+#define HB_ERR_RANGE        6  /* non-finite coordinate met during setpts                */
+#define HB_ERR_WORKSPACE    7  /* caller-provided workspace smaller than required        */
+
+/* ---- enums (values identical to the reference) --------------------------------------- */
+/* nufft_type, cpp/corelib/lib/fft/nufft.cppm:42-48 */
+#define HB_NUFFT_TYPE_1 1      /* BACKWARD / adjoint */
+#define HB_NUFFT_TYPE_2 2      /* FORWARD            */
+/* nufft_method_cuda, cpp/corelib/lib/fft/nufft.cppm:65-70. Every value selects the same
+ * bin-sorted tile kernels here; the value is kept so callers port unchanged. */
+#define HB_METHOD_GM_NO_SORT 0
+#define HB_METHOD_GM_SORT    1
+#define HB_METHOD_SM         2
+#define HB_METHOD_DEFAULT    3
+/* ToeplitzMultType, cpp/corelib/lib/fft/toeplitz.cppm:47-51 */
+#define HB_MULT_NONE      0
+#define HB_MULT_MULT      1
+#define HB_MULT_MULT_CONJ 2
+/* ToeplitzAccumulateType, cpp/corelib/lib/fft/toeplitz.cppm:53-56 */
+#define HB_ACC_NONE       0
+#define HB_ACC_ACCUMULATE 1
+
+/* ---- library ---------------------------------------------------------------------- */
+const char* hb_last_error(void);
+int hb_version(void);
+
+/* ---- NUFFT plan ---------------------------------------------------------------------
+ * Replaces nufft_plan<cuda_t,f32_t,DIM,NT> (cpp/corelib/lib/fft/nufft.cppm:103-310), i.e.
+ * cufinufftf_makeplan / setpts / execute / destroy.
+ *
+ * Kernel: Kaiser-Bessel, phi(z) = I0(beta*sqrt(1-(2z/w)^2)) / I0(beta) on |z| < w/2 (fine
+ * grid units), beta = pi*sqrt((w/sigma)^2 (sigma-1/2)^2 - 0.8). Width w comes from
+ * `kernel_width` when > 0, else from `tol` as w = ceil(log10(10/tol)) (2 <= w <= 16).
+ * Fine grid per dimension: the smallest 2,3,5-smooth multiple of the spread tile edge that
+ * is >= max(upsampfac*N, 2w).
+ */
+typedef struct hb_nufft_plan_s* hb_nufft_plan;
+
+/* nufft_plan::make, nufft.cppm:107-172. nmodes has `dim` entries in image order (dim 0
+ * slowest). sign: +1 / -1, or 0 for the type's default. upsampfac <= 0 means 2.0. */
+int hb_nufft_makeplan(int type, int dim, const int64_t* nmodes, int sign, int ntransf,
+                      float tol, int kernel_width, double upsampfac, int method,
+                      hb_nufft_plan* plan_out);
+
+/* nufft_plan::setpts, nufft.cppm:175-203. Coordinates are device float arrays of length M
+ * (coord1/coord2 NULL below 2/3 dims). The plan keeps its own sorted copy; the caller's
+ * arrays may be freed afterwards. Bin-sorts the points on `stream` and synchronises it once
+ * to size the spread work list. A non-finite coordinate returns HB_ERR_RANGE. */
+int hb_nufft_setpts(hb_nufft_plan plan, int64_t M, const float* coord0, const float* coord1,
+                    const float* coord2, void* stream);
+
+/* nufft_plan::execute, nufft.cppm:205-250.
+ *   type 1: in = c64 [ntransf, M] nonuniform data, out = c64 [ntransf, N0, ..] modes;
+ *   type 2: in = c64 [ntransf, N0, ..] modes,      out = c64 [ntransf, M].
+ * Allocation free, graph capturable. */
+int hb_nufft_execute(hb_nufft_plan plan, const void* in, void* out, void* stream);
+
+/* nufft_plan::free / ~nufft_plan, nufft.cppm:279-301. Safe on NULL. */
+int hb_nufft_destroy(hb_nufft_plan plan);
+
+/* Plan introspection: fine grid sizes (image order), kernel width, beta, device bytes held. */
+int hb_nufft_get_info(hb_nufft_plan plan, int64_t* fine_out3, int* width_out,
+                      double* beta_out, size_t* device_bytes_out);
+
+/* ---- Toeplitz ------------------------------------------------------------------------
+ * toeplitz_kernel, cpp/corelib/lib/fft/nufft.cppm:386-441:
+ *   kernel (shape [2N0, .., 2N{dim-1}], c64) = FFT( embed_{[0,2N-1)}( type1(nudata; 2N-1
+ *   modes) ) ) / prod(N).
+ * nudata is c64 [M] (the reference's [1, M]). The type-1 uses this library's NUFFT with the
+ * given kernel width (<= 0: from tol = 1e-5 as the reference asks for f32).
+ * Allocates and frees a temporary NUFFT plan and grid (not graph capturable). */
+int hb_toeplitz_kernel(int dim, const int64_t* kernel_shape, int64_t M, const float* coord0,
+                       const float* coord1, const float* coord2, const void* nudata,
+                       void* kernel_out, int kernel_width, void* stream);
+
+/* transform_toeplitz_kernel, cpp/corelib/lib/fft/toeplitz.cppm:510-609: re-lays the
+ * straight kernel ([2N..] c64, from hb_toeplitz_kernel) into the layout
+ * hb_toeplitz_multiplication / hb_sense_normal read (same element count, c64), with the
+ * inverse-FFT normalisation 1/prod(2N) folded in. in and out must not alias. */
+int hb_transform_toeplitz_kernel(int dim, const int64_t* kernel_shape, const void* kernel_in,
+                                 void* kernel_out, void* stream);
+
+/* Bytes of device workspace hb_toeplitz_multiplication / hb_sense_normal need for images of
+ * shape `shape` ([N0..], dim entries) with `nbatch` batches (coils). */
+int hb_toeplitz_workspace_size(int dim, const int64_t* shape, int64_t nbatch, size_t* bytes);
+
+/* toeplitz_multiplication / ops_toeplitz_multiplication, cpp/corelib/lib/fft/toeplitz.cppm:
+ * 611-712 and 722-857 (kernel code fft/kernels/toeplitz_load_3D.cu:18-79). For each batch b:
+ *   t      = input[b] * m(mult1, in_m1) * m(mult2, in_m2)
+ *   v      = crop_{[N-1,2N-1)}( IFFT( FFT(pad_{2N}(t)) * K ) )
+ *   v      = v * m(mult1, out_m1) * m(mult2, out_m2) * m(input[b], io_mult)
+ *   out[b] = v (+ out[b] if accumulate)
+ * m(a, NONE) = 1, m(a, MULT) = a, m(a, MULT_CONJ) = conj(a). mult1/mult2 are [N..] or NULL.
+ * kernel is the transformed kernel. `workspace` must hold hb_toeplitz_workspace_size bytes;
+ * NULL makes the call allocate it stream-ordered (cudaMallocAsync) and free it after. */
+int hb_toeplitz_multiplication(int dim, const int64_t* shape, int64_t nbatch,
+                               const void* input, void* output, const void* kernel,
+                               void* workspace, size_t workspace_bytes,
+                               const void* mult1, const void* mult2,
+                               int io_mult, int in_m1, int out_m1, int in_m2, int out_m2,
+                               int accumulate, void* stream);
+
+/* NORMAL_T_T1_OP::operator(), cpp/corelib/lib/mri/normal.cppm:65-88, fused:
+ *   out = sum_c conj(S_c) * T(S_c * x)     (x, out: [N..]; smaps: [C, N..])
+ * with T the Toeplitz operator of `kernel` (transformed). The coil sum happens inside the
+ * last FFT pass; no [C, N..] intermediate is written. out must not alias x.
+ * Workspace as for hb_toeplitz_multiplication with nbatch = C. */
+int hb_sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x,
+                    const void* smaps, const void* kernel, void* out,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- conjugate gradient --------------------------------------------------------------
+ * Vector steps of conjugate_gradient, cpp/corelib/lib/op/cg.cppm:122-184, with all scalars
+ * on the device (no host read per iteration) and every inner product accumulated in FP64
+ * in a fixed order. The state block is opaque device memory of hb_cg_state_bytes() bytes.
+ * An iteration is  Ap = A(p); hb_cg_step(...). Once sqrt(rzold) < tol the steps leave x, r,
+ * p unchanged (the reference breaks out of its loop), so a fixed-length captured loop gives
+ * the reference's result. */
+size_t hb_cg_state_bytes(void);
+/* r = b - Ax; p = r; rzold = Re<r,r>; state.tol = tol. */
+int hb_cg_init(int64_t n, const void* b, const void* Ax, void* r, void* p, void* state,
+               double tol, void* stream);
+/* pAp = Re<p,Ap>; alpha = rzold/pAp; x += alpha p; r -= alpha Ap; rznew = Re<r,r>;
+ * p = r + (rznew/rzold) p; rzold = rznew. */
+int hb_cg_step(int64_t n, void* x, void* r, void* p, const void* Ap, void* state, void* stream);
+/* Copies {rzold, iterations done, converged flag} to host (synchronises the stream). */
+int hb_cg_read_state(const void* state, double* rzold, int64_t* iters, int* converged,
+                     void* stream);
+
+/* ---- vector helpers ------------------------------------------------------------------ */
+/* Re<a,b> in FP64, written to *result_dev (a device double). Deterministic order. */
+int hb_vdot_real(int64_t n, const void* a, const void* b, double* result_dev, void* stream);
+
+/* ---- measurement hooks (no counterpart in the reference) ------------------------------
+ * When enabled, every kernel launch of this library is bracketed by CUDA events on the stream
+ * it runs on. hb_timing_read synchronises on the recorded events, writes the per-kernel-name
+ * summed milliseconds (first-seen order; names '\n'-separated into `names`), the number of
+ * names and of launches recorded, then clears the record. Not for use inside stream capture. */
+int hb_timing_enable(int on);
+int hb_timing_read(char* names, size_t names_cap, float* ms, int cap, int* n_names,
+                   int* n_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HASTY_B200_H */

@@ -1,0 +1,81 @@
+"""Straight Toeplitz kernel / multiply and the SENSE normal operator, restated in numpy (FP64).
+
+- ``toeplitz_kernel``  follows cpp/corelib/lib/fft/nufft.cppm:386-441: type-1 of the sample
+  weights onto 2N-1 modes per axis, embedded at [0, 2N-1) of a 2N grid, FFT, times 1/prod(N).
+- ``toeplitz_multiply`` follows nufft.cppm:448-479: FFT with zero padding to 2N, times the
+  kernel, inverse FFT (normalised), crop [N-1, 2N-1).
+- ``toeplitz_multiplication`` applies the reference's multiply flags exactly as
+  cpp/corelib/lib/fft/kernels/toeplitz_load_3D.cu:2-79 does around that convolution.
+- ``sense_normal`` is NORMAL_T_T1_OP::operator() (cpp/corelib/lib/mri/normal.cppm:65-88):
+  sum_c conj(S_c) T(S_c x).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import gridding, nudft
+
+NONE, MULT, MULT_CONJ = 0, 1, 2
+
+
+def toeplitz_kernel(coords, shape, weights=None, w: int = 6, sigma: float = 2.0, exact: bool = False):
+    """Kernel [2N..] for image shape N. exact=True uses the FP64 NUDFT for the type-1."""
+    shape = tuple(int(s) for s in shape)
+    M = np.asarray(coords[0]).shape[0]
+    nud = np.ones((1, M), dtype=np.complex128) if weights is None else np.asarray(weights, np.complex128).reshape(1, M)
+    nm = tuple(2 * s - 1 for s in shape)
+    if exact:
+        red = nudft.type1(coords, nud, nm, sign=1)[0]
+    else:
+        red = gridding.nufft1(coords, nud, nm, w=w, sigma=sigma, sign=1)[0]
+    k = np.zeros(tuple(2 * s for s in shape), dtype=np.complex128)
+    k[tuple(slice(0, m) for m in nm)] = red
+    return np.fft.fftn(k) / float(np.prod(shape))
+
+
+def toeplitz_multiply(inout, kernel):
+    """inout [B, N..] -> crop(ifftn(fftn(pad 2N) * kernel)) per batch."""
+    inout = np.asarray(inout, dtype=np.complex128)
+    shape = inout.shape[1:]
+    d = len(shape)
+    axes = tuple(range(1, d + 1))
+    mid = np.fft.fftn(inout, s=tuple(2 * s for s in shape), axes=axes)
+    mid = mid * kernel[None]
+    mid = np.fft.ifftn(mid, axes=axes)
+    return mid[(slice(None),) + tuple(slice(s - 1, 2 * s - 1) for s in shape)]
+
+
+def _m(a, b, t):
+    if t == MULT:
+        return a * b
+    if t == MULT_CONJ:
+        return a * np.conj(b)
+    return a
+
+
+def toeplitz_multiplication(inp, out, kernel, mult1=None, mult2=None, io_mult=NONE, in_m1=MULT, out_m1=MULT_CONJ,
+                            in_m2=MULT, out_m2=MULT_CONJ, accumulate=0):
+    """Flag semantics of toeplitz_multiplication with the straight kernel; returns a new array."""
+    inp = np.asarray(inp, dtype=np.complex128)
+    t = inp.copy()
+    if mult1 is not None:
+        t = _m(t, mult1[None], in_m1)
+    if mult2 is not None:
+        t = _m(t, mult2[None], in_m2)
+    v = toeplitz_multiply(t, kernel)
+    if mult1 is not None:
+        v = _m(v, mult1[None], out_m1)
+    if mult2 is not None:
+        v = _m(v, mult2[None], out_m2)
+    if io_mult != NONE:
+        v = _m(v, inp, io_mult)
+    if accumulate:
+        v = v + np.asarray(out, dtype=np.complex128)
+    return v
+
+
+def sense_normal(x, smaps, kernel):
+    x = np.asarray(x, dtype=np.complex128)
+    s = np.asarray(smaps, dtype=np.complex128)
+    v = toeplitz_multiply(s * x[None], kernel)
+    return np.sum(np.conj(s) * v, axis=0)

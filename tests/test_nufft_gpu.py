@@ -1,0 +1,198 @@
+"""NUFFT type 1 / type 2 on the GPU through the C ABI, against the oracle.
+
+Parity bar: relative L2 error <= 1e-5 against the same-algorithm FP64 restatement
+(oracle.gridding); against the FP64 NUDFT the error is the kernel's own accuracy (stated per case).
+"""
+import numpy as np
+import pytest
+
+from helpers import crand, rand_coords, relerr, to_dev, to_np
+from oracle import gridding, kb, nudft
+
+PARITY = 1e-5
+# NUDFT error of the Kaiser-Bessel kernel at sigma = 2 by width (measured on the oracle)
+NUDFT_TOL = {4: 2e-3, 5: 2e-4, 6: 3e-5, 7: 5e-6, 8: 3e-6}
+
+CASES = [
+    # dim, nmodes, M, ntransf, width
+    (1, (37,), 500, 2, 4),
+    (2, (24, 20), 3000, 1, 4),
+    (2, (32, 32), 4000, 3, 6),
+    (2, (17, 30), 2500, 12, 5),
+    (3, (12, 14, 10), 4000, 1, 4),
+    (3, (16, 16, 16), 6000, 8, 4),
+    (3, (16, 12, 20), 5000, 5, 6),
+    (3, (20, 20, 20), 8000, 32, 6),
+    (3, (10, 10, 10), 3000, 40, 7),
+    (3, (24, 24, 24), 6000, 2, 10),
+]
+
+
+def _plan(hb, ntype, nmodes, ntransf, w, sign=None):
+    opts = hb.NufftOpts(nmodes=nmodes, ntransf=ntransf, kernel_width=w, sign=sign)
+    return hb.NufftPlan(ntype, opts)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,nmodes,M,T,w", CASES)
+def test_type1_parity(cuda, dim, nmodes, M, T, w):
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(11 + M)
+    coords = rand_coords(rng, dim, M)
+    c = crand(rng, T, M)
+    plan = _plan(hb, hb.NufftType.TYPE_1, nmodes, T, w)
+    plan.setpts([to_dev(x, cuda) for x in coords])
+    got = to_np(plan(to_dev(c, cuda)))
+    ref = gridding.nufft1(coords, c, nmodes, w=w)
+    e = relerr(got, ref)
+    assert e <= PARITY, f"type1 parity {e:.2e}"
+    if np.prod(nmodes) * M <= 4096 * 8000:
+        ex = nudft.type1(coords, c, nmodes, sign=1)
+        assert relerr(got, ex) <= NUDFT_TOL.get(w, 1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,nmodes,M,T,w", CASES)
+def test_type2_parity(cuda, dim, nmodes, M, T, w):
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(21 + M)
+    coords = rand_coords(rng, dim, M)
+    f = crand(rng, T, *nmodes)
+    plan = _plan(hb, hb.NufftType.TYPE_2, nmodes, T, w)
+    plan.setpts([to_dev(x, cuda) for x in coords])
+    got = to_np(plan(to_dev(f, cuda)))
+    ref = gridding.nufft2(coords, f, w=w)
+    e = relerr(got, ref)
+    assert e <= PARITY, f"type2 parity {e:.2e}"
+    if np.prod(nmodes) * M <= 4096 * 8000:
+        ex = nudft.type2(coords, f, sign=-1)
+        assert relerr(got, ex) <= NUDFT_TOL.get(w, 1e-6)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sign", [1, -1])
+def test_signs(cuda, sign):
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(5)
+    nm, M = (12, 10, 8), 2000
+    coords = rand_coords(rng, 3, M)
+    c = crand(rng, 2, M)
+    p1 = _plan(hb, hb.NufftType.TYPE_1, nm, 2, 6, sign=sign)
+    p1.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p1(to_dev(c, cuda))), nudft.type1(coords, c, nm, sign=sign)) <= NUDFT_TOL[6]
+    f = crand(rng, 2, *nm)
+    p2 = _plan(hb, hb.NufftType.TYPE_2, nm, 2, 6, sign=sign)
+    p2.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p2(to_dev(f, cuda))), nudft.type2(coords, f, sign=sign)) <= NUDFT_TOL[6]
+
+
+@pytest.mark.gpu
+def test_adjointness(cuda):
+    """<A f, c> == <f, A^H c> for the type-2 / type-1 pair on the same points."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(8)
+    nm, M, T = (16, 16, 16), 7000, 3
+    coords = rand_coords(rng, 3, M)
+    f, c = crand(rng, T, *nm), crand(rng, T, M)
+    p1 = _plan(hb, hb.NufftType.TYPE_1, nm, T, 6)
+    p2 = _plan(hb, hb.NufftType.TYPE_2, nm, T, 6)
+    for p in (p1, p2):
+        p.setpts([to_dev(x, cuda) for x in coords])
+    Af = to_np(p2(to_dev(f, cuda))).astype(np.complex128)
+    Ahc = to_np(p1(to_dev(c, cuda))).astype(np.complex128)
+    lhs = np.vdot(c, Af)
+    rhs = np.vdot(Ahc, f)
+    assert abs(lhs - rhs) / (np.linalg.norm(Af) * np.linalg.norm(c)) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_coordinates_outside_pi(cuda):
+    """Coordinates are periodic: x and x + 2 pi m give the same transform."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(9)
+    nm, M = (16, 16), 3000
+    coords = rand_coords(rng, 2, M)
+    shifted = [(x + 2 * np.pi * rng.integers(-3, 4, M)).astype(np.float32) for x in coords]
+    c = crand(rng, 1, M)
+    p = _plan(hb, hb.NufftType.TYPE_1, nm, 1, 6)
+    p.setpts([to_dev(x, cuda) for x in shifted])
+    got = to_np(p(to_dev(c, cuda)))
+    ref = gridding.nufft1(shifted, c, nm, w=6)
+    assert relerr(got, ref) <= PARITY
+    assert relerr(got, nudft.type1(coords, c, nm)) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_dense_center_and_edges(cuda):
+    """Heavy tiles (many points in one bin, split into subproblems) and points on the grid edge."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(10)
+    nm = (20, 20, 20)
+    M1 = 30000
+    center = [rng.normal(0, 0.05, M1).astype(np.float32) for _ in range(3)]
+    edge = [np.full(500, -np.pi, np.float32), np.full(500, np.float32(np.pi) * np.float32(0.9999999)),
+            rng.uniform(-np.pi, np.pi, 500).astype(np.float32)]
+    coords = [np.concatenate([a, b]) for a, b in zip(center, edge)]
+    M = coords[0].shape[0]
+    c = crand(rng, 4, M)
+    p = _plan(hb, hb.NufftType.TYPE_1, nm, 4, 6)
+    p.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p(to_dev(c, cuda))), gridding.nufft1(coords, c, nm, w=6)) <= PARITY
+    f = crand(rng, 4, *nm)
+    q = _plan(hb, hb.NufftType.TYPE_2, nm, 4, 6)
+    q.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(q(to_dev(f, cuda))), gridding.nufft2(coords, f, w=6)) <= PARITY
+
+
+@pytest.mark.gpu
+def test_empty_points(cuda):
+    import torch
+    import hastycucompute_b200 as hb
+    nm = (8, 8, 8)
+    p = _plan(hb, hb.NufftType.TYPE_1, nm, 2, 4)
+    z = torch.zeros(0, dtype=torch.float32, device=cuda)
+    p.setpts([z, z, z])
+    out = p(torch.zeros((2, 0), dtype=torch.complex64, device=cuda))
+    assert torch.count_nonzero(out).item() == 0
+    q = _plan(hb, hb.NufftType.TYPE_2, nm, 2, 4)
+    q.setpts([z, z, z])
+    assert q(torch.ones((2, *nm), dtype=torch.complex64, device=cuda)).shape == (2, 0)
+
+
+@pytest.mark.gpu
+def test_nonfinite_coordinate_is_an_error(cuda):
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(3)
+    coords = rand_coords(rng, 2, 100)
+    coords[1][17] = np.nan
+    p = _plan(hb, hb.NufftType.TYPE_1, (8, 8), 1, 4)
+    with pytest.raises(hb.HastyError, match="HB_ERR_RANGE"):
+        p.setpts([to_dev(x, cuda) for x in coords])
+    with pytest.raises(RuntimeError):
+        p(to_dev(crand(rng, 1, 100), cuda))
+
+
+@pytest.mark.gpu
+def test_plan_reuse_and_resetpts(cuda):
+    """setpts twice on one plan (growing and shrinking M) gives fresh results."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(4)
+    nm = (12, 12, 12)
+    p = _plan(hb, hb.NufftType.TYPE_2, nm, 3, 5)
+    f = crand(rng, 3, *nm)
+    for M in (1000, 5000, 300):
+        coords = rand_coords(rng, 3, M)
+        p.setpts([to_dev(x, cuda) for x in coords])
+        assert relerr(to_np(p(to_dev(f, cuda))), gridding.nufft2(coords, f, w=5)) <= PARITY
+
+
+@pytest.mark.gpu
+def test_plan_info_matches_oracle_grid(cuda):
+    import hastycucompute_b200 as hb
+    for nm, w in [((64, 64, 64), 4), ((160, 160, 160), 6), ((256, 256), 4), ((319, 319, 319), 6)]:
+        p = _plan(hb, hb.NufftType.TYPE_1, nm, 1, w)
+        info = p.info()
+        assert info.fine == kb.fine_grid(nm, w)
+        assert info.width == w
+        assert abs(info.beta - kb.beta(w)) < 1e-9
+        p.free()

@@ -1,0 +1,123 @@
+"""Toeplitz kernel build, fused multiplication (all reference flag combinations) and the SENSE
+normal operator on the GPU through the C ABI, against the oracle. Bar: relative L2 <= 1e-5."""
+import itertools
+
+import numpy as np
+import pytest
+
+from helpers import crand, rand_coords, relerr, to_dev, to_np
+from oracle import refload
+from oracle import toeplitz as otp
+
+PARITY = 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,M,w", [((12, 10), 3000, 4), ((16, 16), 5000, 6), ((8, 10, 12), 4000, 4),
+                                        ((16, 16, 16), 8000, 6)])
+def test_toeplitz_kernel(cuda, shape, M, w):
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(M)
+    coords = rand_coords(rng, len(shape), M)
+    wts = rng.uniform(0.5, 1.5, M).astype(np.float32)
+    K = hb.build_toeplitz_kernel([to_dev(c, cuda) for c in coords], shape, to_dev(wts, cuda), kernel_width=w)
+    ref = otp.toeplitz_kernel(coords, shape, wts, w=w)
+    assert relerr(to_np(K), ref) <= PARITY
+    # and the kernel is the NUDFT one up to the NUFFT accuracy
+    if np.prod(shape) <= 4096:
+        ex = otp.toeplitz_kernel(coords, shape, wts, exact=True)
+        assert relerr(to_np(K), ex) <= {4: 2e-3, 6: 3e-5}[w]
+
+
+FLAGS = [
+    (0, 1, 2, 1, 2, 0),  # the reference defaults
+    (2, 1, 0, 0, 0, 0),  # NORMAL_T_T1_OP
+    (0, 1, 2, 0, 0, 0),  # NORMAL_T_T2_OP
+    (0, 1, 2, 1, 2, 1),
+    (1, 2, 1, 2, 1, 1),
+    (0, 0, 0, 0, 0, 0),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(6, 8, 10), (16, 16, 16), (12, 10), (32, 30)])
+@pytest.mark.parametrize("flags", FLAGS)
+@pytest.mark.parametrize("use_m2", [False, True])
+def test_multiplication_flags(cuda, shape, flags, use_m2):
+    import torch
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(hash((shape, flags, use_m2)) % 2**32)
+    B = 3
+    inp = crand(rng, B, *shape)
+    out0 = crand(rng, B, *shape)
+    m1 = crand(rng, *shape)
+    m2 = crand(rng, *shape) if use_m2 else None
+    K = crand(rng, *[2 * s for s in shape]).astype(np.complex128)
+    io, i1, o1, i2, o2, acc = flags
+    ref = otp.toeplitz_multiplication(inp, out0, K, m1, m2, io, i1, o1, i2, o2, acc)
+    Kt = hb.transform_toeplitz_kernel(to_dev(K.astype(np.complex64), cuda))
+    out = to_dev(out0, cuda)
+    hb.toeplitz_multiplication(to_dev(inp, cuda), out, Kt, None, to_dev(m1, cuda),
+                               to_dev(m2, cuda) if use_m2 else None, io, i1, o1, i2, o2, acc)
+    assert relerr(to_np(out), ref) <= PARITY
+    if refload.available():
+        r2 = refload.multiplication(inp, out0, K, m1, m2, io, i1, o1, i2, o2, acc)
+        assert relerr(to_np(out), r2) <= PARITY
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,C", [((16, 16, 16), 8), ((20, 18, 16), 32), ((10, 12, 14), 40), ((64, 64), 12),
+                                     ((24, 40), 3)])
+def test_sense_normal(cuda, shape, C):
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import synthetic
+    rng = np.random.default_rng(C)
+    x = crand(rng, *shape)
+    S = synthetic.coil_maps(C, shape)
+    K = crand(rng, *[2 * s for s in shape]).astype(np.complex128)
+    op = hb.NormalTT1Op(to_dev(K.astype(np.complex64), cuda), to_dev(S, cuda))
+    got = to_np(op(to_dev(x, cuda)))
+    ref = otp.sense_normal(x, S, K)
+    assert relerr(got, ref) <= PARITY
+    # equals the flat multiplication with the NORMAL_T_T1_OP flags followed by the coil sum
+    flat = otp.toeplitz_multiplication(S, np.zeros_like(S), K, x, None, 2, 1, 0, 0, 0, 0).sum(0)
+    assert relerr(got, flat) <= PARITY
+
+
+@pytest.mark.gpu
+def test_sense_normal_is_scaled_AhA(cuda):
+    """T = (1/n) A^H diag(w) A: the fused normal op equals the plain SENSE pair up to NUFFT error."""
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import synthetic
+    rng = np.random.default_rng(2)
+    shape, C, M, w = (16, 16, 16), 8, 12000, 6
+    coords = rand_coords(rng, 3, M)
+    S = synthetic.coil_maps(C, shape)
+    x = crand(rng, *shape)
+    dc = [to_dev(c, cuda) for c in coords]
+    K = hb.build_toeplitz_kernel(dc, shape, kernel_width=w)
+    op = hb.NormalTT1Op(K, to_dev(S, cuda))
+    got = to_np(op(to_dev(x, cuda)))
+    sense = hb.SenseOp(dc, to_dev(S, cuda), kernel_width=w)
+    plain = to_np(sense.normal(to_dev(x, cuda))) / np.prod(shape)
+    assert relerr(got, plain) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_workspace_argument(cuda):
+    import torch
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import toeplitz as tp
+    rng = np.random.default_rng(0)
+    shape, B = (8, 8, 8), 2
+    inp = crand(rng, B, *shape)
+    K = crand(rng, 16, 16, 16)
+    Kt = hb.transform_toeplitz_kernel(to_dev(K, cuda))
+    ws = tp.make_workspace(shape, B, cuda)
+    out = torch.zeros((B, *shape), dtype=torch.complex64, device=cuda)
+    hb.toeplitz_multiply(to_dev(inp, cuda), Kt, ws)
+    small = torch.empty(10, dtype=torch.complex64, device=cuda)
+    with pytest.raises(hb.HastyError, match="WORKSPACE"):
+        hb.toeplitz_multiplication(to_dev(inp, cuda), out, Kt, small)
+    with pytest.raises(hb.HastyError, match="INVALID_ARG"):
+        hb.toeplitz_multiplication(to_dev(inp, cuda), out, Kt, None, None, None, 3)
