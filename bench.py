@@ -1,0 +1,481 @@
+#!/usr/bin/env python
+"""Benchmark of the Toeplitz SENSE normal operator (A^H A), the NUFFT pair and CG.
+
+Workload (default, one GPU): 160^3 complex64 image, 32 coils, 3-D cones-like spirals with 24000
+interleaves x 256 samples (6,144,000 points), |k|^2 density compensation, Kaiser-Bessel width 6,
+upsampling 2. Seeded synthetic data, built on the host.
+
+A "step" is one A^H A apply (x -> sum_c conj(S_c) T(S_c x)), the body of the CG loop. `value` is
+applies/s over all ranks with the inputs resident in HBM; `e2e` is the same apply through the
+public operator with the image copied in from pinned host memory and the result copied back
+inside the timed region. The NUFFT type-1 / type-2 throughput (Msamp/s = M * coils / s) and the
+graph-captured 20-iteration CG recon rate are reported beside it.
+
+Multi-GPU (torchrun): every rank runs its own replica (frames are independent; no collective
+on the data path), so scaling is weak and `value` sums the ranks' work over the slowest rank's
+time.
+
+--impl reference times the reference-side CPU implementation (the oracle restatement of the
+straight Toeplitz SENSE normal operator, cpp/corelib/lib/fft/nufft.cppm:448-479 +
+cpp/corelib/lib/mri/normal.cppm:65-88, multithreaded FFT) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "A^HA applies/s, NUFFT Msamp/s; batched vs looped CG recons/s @1e-5 rel err"
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+
+
+# ---------------------------------------------------------------------------------------------
+# workload
+
+WORKLOADS = {
+    # name: (image shape, coils, trajectory kind, (interleaves, samples), width, dcf, cg iterations)
+    "cones160": ((160, 160, 160), 32, "cones", (24000, 256), 6, True, 20),
+    "radial64": ((64, 64, 64), 8, "radial", (1024, 128), 4, False, 10),
+    # profiling size: pass buffers (~450 MB) larger than L2, a few GB on the device in total
+    "radial96": ((96, 96, 96), 16, "radial", (2048, 192), 6, False, 10),
+}
+
+
+def make_workload(name: str):
+    from hastycucompute_b200 import synthetic
+
+    shape, C, kind, (ni, ns), w, use_dcf, iters = WORKLOADS[name]
+    if kind == "cones":
+        coords = synthetic.cones_spiral(ni, ns)
+    else:
+        coords = synthetic.golden_means_radial(ni, ns)
+    dcf = synthetic.dcf_k2(coords) if use_dcf else None
+    smaps = synthetic.coil_maps(C, shape)
+    x = synthetic.image(shape)
+    return dict(name=name, shape=shape, C=C, coords=coords, dcf=dcf, smaps=smaps, x=x, w=w, iters=iters,
+                M=coords.shape[1])
+
+
+def peaks():
+    if MEASURED_PEAKS.exists():
+        d = json.loads(MEASURED_PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing
+
+def dist_setup(use_gpu: bool):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if use_gpu else "gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int, device) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# reference arm: CPU restatement on the host cores
+
+def run_reference(args, wl_name: str):
+    world, rank, _ = dist_setup(False)
+    if rank != 0:
+        return 0
+    from oracle import toeplitz as otp
+
+    wl = make_workload_cpu_only(wl_name)
+    shape, C = wl["shape"], wl["C"]
+    cores = len(os.sched_getaffinity(0))
+    rng = np.random.default_rng(7)
+    # a random Hermitian-structured kernel stands in for the built one: the apply's cost does
+    # not depend on its values
+    K = (rng.standard_normal(tuple(2 * s for s in shape)) + 1j * rng.standard_normal(tuple(2 * s for s in shape))).astype(np.complex64)
+    coils_per_step = 1
+    times = []
+    for it in range(args.warmup + args.steps):
+        c0 = it % C
+        t0 = time.perf_counter()
+        otp.sense_normal(wl["x"], wl["smaps"][c0:c0 + coils_per_step], K, workers=cores, dtype=np.complex64)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+    per_apply = statistics.mean(times) * C / coils_per_step
+    value = 1.0 / per_apply
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "applies/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_apply * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(wl),
+        "cpu_baseline": {"value": value, "unit": "applies/s", "cores": cores, "kind": "port",
+                         "sample": f"{coils_per_step} of {C} coils per step (straight Toeplitz SENSE normal, "
+                                   f"scipy FFT on {cores} threads), scaled to a full apply"},
+        "e2e": {"value": value, "unit": "applies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def make_workload_cpu_only(name):
+    return make_workload(name)
+
+
+def workload_config(wl):
+    return {
+        "workload": f"toeplitz_sense_normal_{wl['name']}",
+        "image": list(wl["shape"]), "coils": wl["C"], "samples": int(wl["M"]), "kernel": "kaiser-bessel",
+        "kernel_width": wl["w"], "upsampfac": 2.0, "dcf": "|k|^2" if wl["dcf"] is not None else "none",
+        "cg_iterations": wl["iters"], "parallelism": "replicas (one frame per rank)",
+        "l2": "inputs larger than L2 (coil maps + workspace >> 126 MB)",
+    }
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+
+def aha_bytes(n: int, C: int, dim: int = 3) -> dict:
+    """Algorithmic HBM bytes per pass of one fused apply (c64 = 8 B, n voxels, C coils)."""
+    if dim == 3:
+        return {"toeplitz P1": 8 * n * (3 * C) + 8 * n, "toeplitz P2": 8 * n * 6 * C,
+                "toeplitz P3": 8 * n * 8 * C + 8 * n * 8, "toeplitz P4": 8 * n * 6 * C,
+                "toeplitz P5 sense": 8 * n * 3 * C + 8 * n}
+    return {}
+
+
+def run_ours(args, wl_name: str):
+    import torch
+
+    world, rank, local = dist_setup(True)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import _lib
+
+    wl = make_workload(wl_name)
+    shape, C, M, w = wl["shape"], wl["C"], wl["M"], wl["w"]
+    n = int(np.prod(shape))
+    coords = [torch.from_numpy(np.ascontiguousarray(c)).to(dev) for c in wl["coords"]]
+    dcf = torch.from_numpy(wl["dcf"]).to(dev) if wl["dcf"] is not None else None
+    smaps = torch.from_numpy(wl["smaps"]).to(dev)
+    x = torch.from_numpy(wl["x"]).to(dev)
+
+    t0 = time.perf_counter()
+    K = hb.build_toeplitz_kernel(coords, shape, dcf, kernel_width=w)
+    torch.cuda.synchronize()
+    t_kernel = time.perf_counter() - t0
+    op = hb.NormalTT1Op(K, smaps)
+    out = torch.empty_like(x)
+
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        op.apply(x, out)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K applies, inputs resident -----------------------------------------
+    _lib.timing_enable(True)
+    _lib.timing_read()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            op.apply(x, out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    per_kernel, launches = _lib.timing_read()
+    _lib.timing_enable(False)
+    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(ms, world, dev)
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel
+    hbm_peak, peak_kind = peaks()
+    bytes_per = aha_bytes(n, C, len(shape))
+    kname = max(per_kernel, key=per_kernel.get)
+    k_ms = per_kernel[kname] / args.steps
+    algo = bytes_per.get(kname, 0)
+    achieved = algo / (k_ms / 1e3) / 1e9
+    roofline = {"kernel": kname, "bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "peak_kind": peak_kind,
+                "traffic": None, "algorithmic_bytes": algo, "avg_ms": round(k_ms, 4),
+                "share": round(per_kernel[kname] / sum(per_kernel.values()), 4)}
+    apply_bytes = 8 * n * (26 * C + 10)
+    aha_roof = {"bytes_model": apply_bytes, "achieved_gbs": round(apply_bytes / (ms_step / 1e3) / 1e9, 1),
+                "frac": round(apply_bytes / (ms_step / 1e3) / 1e9 / hbm_peak, 4),
+                "per_kernel_ms": {k: round(v / args.steps, 4) for k, v in per_kernel.items()}}
+
+    # ---- e2e: host image in, host result out, through the public operator ------------------
+    xh = torch.from_numpy(wl["x"]).pin_memory()
+    oh = torch.empty_like(xh).pin_memory()
+    xd = torch.empty_like(x)
+    for _ in range(2):
+        xd.copy_(xh, non_blocking=True)
+        op.apply(xd, out)
+        oh.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0.record(stream)
+    for _ in range(args.steps):
+        xd.copy_(xh, non_blocking=True)
+        op.apply(xd, out)
+        oh.copy_(out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    e2e = {"value": world * args.steps / (e2e_ms / 1e3), "unit": "applies/s",
+           "h2d_bytes_per_step": xh.numel() * 8, "d2h_bytes_per_step": oh.numel() * 8}
+
+    extra = {}
+    # ---- NUFFT pair ----------------------------------------------------------------------------
+    if not args.no_nufft:
+        extra["nufft"] = bench_nufft(args, hb, _lib, coords, wl, dev, stream, hbm_peak)
+    # ---- CG recon, graph captured --------------------------------------------------------------
+    if not args.no_cg:
+        solver = hb.CGSolver(lambda v, o: op.apply(v, o), shape, dev, max_iter=wl["iters"], tol=0.0, graph=True)
+        b = out.clone()
+        solver.solve(torch.zeros_like(x), b)  # capture + warm
+        torch.cuda.synchronize()
+        e0.record(stream)
+        reps = 2
+        for _ in range(reps):
+            solver.solve(torch.zeros_like(x), b)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        cg_ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / reps
+        extra["cg"] = {"recons_per_s": round(world * 1e3 / cg_ms, 3), "iterations": wl["iters"],
+                       "ms_per_recon": round(cg_ms, 3), "graph_captured": True}
+
+    # ---- accuracy of the timed apply: coil subset against the FP64 oracle ------------------------
+    acc = {}
+    if rank == 0 and not args.no_check:
+        acc = check_accuracy(hb, wl, K, dev)
+
+    # ---- CPU baseline (rank 0, N = 1 only) ------------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl, K)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "applies/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(wl), "e2e": e2e,
+            "gpu_launches": launches, "roofline": roofline, "aha_roofline": aha_roof,
+            "cpu_baseline": cpu, "clocks": clk.summary(), "setup": {"toeplitz_kernel_s": round(t_kernel, 3)},
+            "accuracy": acc,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def bench_nufft(args, hb, _lib, coords, wl, dev, stream, hbm_peak):
+    import torch
+    shape, C, M, w = wl["shape"], wl["C"], wl["M"], wl["w"]
+    opts = hb.NufftOpts(nmodes=shape, ntransf=C, kernel_width=w)
+    p2 = hb.NufftPlan(hb.NufftType.TYPE_2, opts)
+    p2.setpts(coords)
+    f = torch.from_numpy(wl["smaps"]).to(dev) * torch.from_numpy(wl["x"]).to(dev)[None]
+    y = torch.empty((C, M), dtype=torch.complex64, device=dev)
+    p1 = hb.NufftPlan(hb.NufftType.TYPE_1, opts)
+    p1.setpts(coords)
+    g = torch.empty_like(f)
+    res = {}
+    nf = p1.info().fine
+    n_os = int(np.prod(nf))
+    d = len(shape)
+    for name, plan, a, b in (("type2", p2, f, y), ("type1", p1, y, g)):
+        for _ in range(2):
+            plan.execute(a, b)
+        torch.cuda.synchronize()
+        _lib.timing_enable(True)
+        _lib.timing_read()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(3, args.steps // 4)
+        e0.record(stream)
+        for _ in range(reps):
+            plan.execute(a, b)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pk, _ = _lib.timing_read()
+        _lib.timing_enable(False)
+        ms = e0.elapsed_time(e1) / reps
+        res[name] = {"msamp_per_s": round(M * C / (ms / 1e3) / 1e6, 1), "ms": round(ms, 3),
+                     "per_kernel_ms": {k: round(v / reps, 4) for k, v in pk.items()}}
+        gk = "interp" if name == "type2" else "spread"
+        if gk in pk:
+            kms = (pk[gk] + pk.get("spread_dense", 0.0)) / reps if gk == "spread" else pk[gk] / reps
+            algo = 4 * d * M + C * (8 * M + 8 * n_os)
+            res[name]["gridding_roofline"] = {"kernel": gk, "algorithmic_bytes": algo,
+                                              "achieved_gbs": round(algo / (kms / 1e3) / 1e9, 1),
+                                              "frac": round(algo / (kms / 1e3) / 1e9 / hbm_peak, 4),
+                                              "avg_ms": round(kms, 4)}
+    # spot checks against the FP64 NUDFT (bounded: 48 points / 48 modes)
+    from oracle import nudft
+    rng = np.random.default_rng(4)
+    pts = rng.choice(M, 48, replace=False)
+    f_np = f[:2].cpu().numpy()
+    y_ref = nudft.type2_at(wl["coords"], f_np, pts, sign=-1)
+    y_got = y[:2].cpu().numpy()[:, pts]
+    res["type2"]["rel_err_vs_nudft"] = float(np.linalg.norm(y_got - y_ref) / np.linalg.norm(y_ref))
+    idx = np.stack([rng.integers(0, s, 48) for s in shape], axis=1)
+    y_np = y[:1].cpu().numpy()
+    g_ref = nudft.type1_at(wl["coords"], y_np, shape, idx, sign=1)
+    g_got = g[:1].cpu().numpy()[(slice(None),) + tuple(idx[:, i] for i in range(d))]
+    res["type1"]["rel_err_vs_nudft"] = float(np.linalg.norm(g_got - g_ref) / np.linalg.norm(g_ref))
+    p1.free()
+    p2.free()
+    return res
+
+
+def check_accuracy(hb, wl, K, dev):
+    """Runs the fused apply on a 2-coil subset and compares it with the FP64 oracle apply using
+    the same kernel."""
+    import torch
+    from oracle import toeplitz as otp
+    sub = wl["smaps"][:2]
+    op2 = hb.NormalTT1Op(K, torch.from_numpy(sub).to(dev))
+    got = op2(torch.from_numpy(wl["x"]).to(dev)).cpu().numpy()
+    Kn = K.cpu().numpy().astype(np.complex128)
+    cores = len(os.sched_getaffinity(0))
+    ref = otp.sense_normal(wl["x"], sub, Kn, workers=cores)
+    return {"aha_rel_err_vs_fp64_oracle": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+            "coils_checked": 2}
+
+
+def cpu_baseline(wl, K):
+    from oracle import toeplitz as otp
+    import torch
+    cores = len(os.sched_getaffinity(0))
+    Kn = K.cpu().numpy()
+    C = wl["C"]
+    # bounded sample: 1 coil, twice; scaled to a full apply
+    times = []
+    for c0 in range(2):
+        t0 = time.perf_counter()
+        otp.sense_normal(wl["x"], wl["smaps"][c0:c0 + 1], Kn, workers=cores, dtype=np.complex64)
+        times.append(time.perf_counter() - t0)
+    per_apply = min(times) * C
+    return {"value": round(1.0 / per_apply, 5), "unit": "applies/s", "cores": cores, "kind": "port",
+            "sample": f"1 of {C} coils (straight Toeplitz SENSE normal, scipy FFT on {cores} threads), "
+                      f"scaled to a full apply"}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cones160")
+    ap.add_argument("--no-nufft", action="store_true")
+    ap.add_argument("--no-cg", action="store_true")
+    ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args, args.workload)
+    return run_ours(args, args.workload)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

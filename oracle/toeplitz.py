@@ -33,15 +33,24 @@ def toeplitz_kernel(coords, shape, weights=None, w: int = 6, sigma: float = 2.0,
     return np.fft.fftn(k) / float(np.prod(shape))
 
 
-def toeplitz_multiply(inout, kernel):
-    """inout [B, N..] -> crop(ifftn(fftn(pad 2N) * kernel)) per batch."""
-    inout = np.asarray(inout, dtype=np.complex128)
+def toeplitz_multiply(inout, kernel, workers: int | None = None, dtype=np.complex128):
+    """inout [B, N..] -> crop(ifftn(fftn(pad 2N) * kernel)) per batch.
+
+    ``workers`` > 1 runs scipy's multithreaded FFT (the timed CPU baseline); ``dtype`` is the
+    working precision (complex128 for parity checks)."""
+    inout = np.asarray(inout, dtype=dtype)
     shape = inout.shape[1:]
     d = len(shape)
     axes = tuple(range(1, d + 1))
-    mid = np.fft.fftn(inout, s=tuple(2 * s for s in shape), axes=axes)
-    mid = mid * kernel[None]
-    mid = np.fft.ifftn(mid, axes=axes)
+    if workers and workers > 1:
+        import scipy.fft as sf
+        mid = sf.fftn(inout, s=tuple(2 * s for s in shape), axes=axes, workers=workers)
+        mid *= kernel[None].astype(dtype, copy=False)
+        mid = sf.ifftn(mid, axes=axes, workers=workers, overwrite_x=True)
+    else:
+        mid = np.fft.fftn(inout, s=tuple(2 * s for s in shape), axes=axes)
+        mid = mid * kernel[None]
+        mid = np.fft.ifftn(mid, axes=axes)
     return mid[(slice(None),) + tuple(slice(s - 1, 2 * s - 1) for s in shape)]
 
 
@@ -74,8 +83,8 @@ def toeplitz_multiplication(inp, out, kernel, mult1=None, mult2=None, io_mult=NO
     return v
 
 
-def sense_normal(x, smaps, kernel):
-    x = np.asarray(x, dtype=np.complex128)
-    s = np.asarray(smaps, dtype=np.complex128)
-    v = toeplitz_multiply(s * x[None], kernel)
+def sense_normal(x, smaps, kernel, workers: int | None = None, dtype=np.complex128):
+    x = np.asarray(x, dtype=dtype)
+    s = np.asarray(smaps, dtype=dtype)
+    v = toeplitz_multiply(s * x[None], kernel, workers=workers, dtype=dtype)
     return np.sum(np.conj(s) * v, axis=0)
