@@ -48,8 +48,10 @@ WORKLOADS = {
     # name: (image shape, coils, trajectory kind, (interleaves, samples), width, dcf, cg iterations)
     "cones160": ((160, 160, 160), 32, "cones", (24000, 256), 6, True, 20),
     "radial64": ((64, 64, 64), 8, "radial", (1024, 128), 4, False, 10),
-    # profiling size: pass buffers (~450 MB) larger than L2, a few GB on the device in total
+    # profiling sizes: pass buffers larger than L2 (126 MB), a few GB on the device in total
     "radial96": ((96, 96, 96), 16, "radial", (2048, 192), 6, False, 10),
+    "prof160": ((160, 160, 160), 8, "cones", (6000, 256), 6, True, 20),
+    "prof96c32": ((96, 96, 96), 32, "radial", (4096, 192), 6, False, 10),
 }
 
 

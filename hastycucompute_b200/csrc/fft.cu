@@ -70,8 +70,7 @@ void pass_setup(PassCfg* c, const FftLen& f, int64_t A, int64_t E, int Lin, int 
     c->out_shift = out_shift;
     c->A = A;
     c->E = E;
-    int W = pass_columns_for(f.L);
-    if (max_cols > 0 && W > max_cols) W = max_cols;
+    const int W = max_cols > 0 ? max_cols : pass_columns_for(f.L);
     int Eb = (int)(E < W ? E : W);
     if (Eb < 1) Eb = 1;
     int Ab = W / Eb;

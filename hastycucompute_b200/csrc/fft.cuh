@@ -52,7 +52,8 @@ struct PassCfg {
 // Chooses the columns per CTA for length L so that two CTAs fit on an SM.
 int pass_columns_for(int L);
 
-// Fills the block decomposition of cfg for extents (A, E) and length information.
+// Fills the block decomposition of cfg for extents (A, E) and length information. max_cols > 0
+// fixes the columns per CTA (the register kernel); otherwise they follow the shared budget.
 void pass_setup(PassCfg* c, const FftLen& f, int64_t A, int64_t E, int Lin, int in_shift,
                 int Lout, int out_shift, int inverse, int max_cols = 0);
 

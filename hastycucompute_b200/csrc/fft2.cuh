@@ -1,0 +1,312 @@
+// Two-level register FFT pass (L = P * Q) for the lengths the hot path uses.
+//
+// For one column x[0..L), with n = t + Q j and k = k1 + P k2 (t, k2 < Q; j, k1 < P):
+//     X[k1 + P k2] = sum_t W_Q^{t k2} [ W_L^{t k1} sum_j x[t + Q j] W_P^{j k1} ]
+// Step 1: thread t loads its P samples straight from global memory into registers, runs the
+// P-point DFT, applies the twiddles W_L^{t k1} and writes one row of the shared transpose.
+// Step 2: thread k1 reads its Q values, runs the Q-point DFT and stores X[k1 + P k2] directly.
+// One shared-memory round trip per transform, P (or Q) independent global accesses per thread.
+// A CTA handles CW columns; the pruned load / store position maps are those of fft.cuh.
+//
+// Fused kernel passes (forward, multiply, inverse) continue from step 2 without a transpose:
+// thread k1 multiplies by the kernel, runs the inverse Q-point DFT over k2, twiddles by
+// W_L^{-n2 k1}, and after one more transpose thread n2 runs the inverse P-point DFT giving
+// x[n2 + Q n1].
+#pragma once
+
+#include "fft.cuh"
+
+namespace hb {
+
+#ifdef __CUDACC__
+
+template <int R>
+struct IsBaseRadix {
+    static constexpr bool value = R == 1 || R == 2 || R == 3 || R == 4 || R == 5 || R == 7 || R == 8;
+};
+
+// first factor used to split a composite register DFT
+template <int R>
+constexpr int split_factor() {
+    return (R % 4 == 0) ? 4 : (R % 2 == 0) ? 2 : (R % 3 == 0) ? 3 : (R % 5 == 0) ? 5 : 7;
+}
+
+// W_L^m from the shared table (exp(-2 pi i m / L)), conjugated for the inverse
+template <bool INV>
+__device__ __forceinline__ float2 tw_get(const float2* tw, int m) {
+    float2 w = tw[m];
+    if (INV) w.y = -w.y;
+    return w;
+}
+
+// In-register DFT of size R; `tws` = L / R so that W_R^m = tw[m * tws].
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg(float2* v, const float2* tw, int tws) {
+    if constexpr (R == 1) {
+        return;
+    } else if constexpr (IsBaseRadix<R>::value) {
+        dft<R, INV>(v);
+    } else {
+        constexpr int A = split_factor<R>();
+        constexpr int B = R / A;
+        float2 y[R];
+#pragma unroll
+        for (int t = 0; t < B; ++t) {
+            float2 a[A];
+#pragma unroll
+            for (int j = 0; j < A; ++j) a[j] = v[t + B * j];
+            dft<A, INV>(a);
+#pragma unroll
+            for (int k1 = 0; k1 < A; ++k1) y[t * A + k1] = (t * k1 == 0) ? a[k1] : cmul(a[k1], tw_get<INV>(tw, t * k1 * tws));
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) {
+            float2 b[B];
+#pragma unroll
+            for (int t = 0; t < B; ++t) b[t] = y[t * A + k1];
+            dft_reg<B, INV>(b, tw, tws * A);
+#pragma unroll
+            for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = b[k2];
+        }
+    }
+}
+
+constexpr int kCW = 16;  // columns per CTA
+
+// Op contract (in addition to fft.cuh's):
+//   static constexpr bool kStoreLFast    // destination contiguous along the output index
+//   static constexpr bool kSenseReduce   // sum over inner columns into one output row
+//   void store(int64_t a, int o, int64_t e, float2 v) const
+//   float2 product(int64_t a, int o, int64_t e, float2 v) const        (kSenseReduce)
+//   void write_row(int64_t a, int o, float2 v) const                   (kSenseReduce)
+template <int P, int Q, class Op>
+__global__ void __launch_bounds__(Q* kCW) pass2_kernel(const Op op, const PassCfg c) {
+    constexpr int L = P * Q;
+    constexpr int CWp = kCW + 1;
+    extern __shared__ float2 smem2[];
+    float2* tw = smem2;       // L
+    float2* Y = smem2 + L;    // [L][CWp] transpose buffer
+    float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][Lout] running sums
+
+    for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = c.tw[i];
+
+    int64_t ab, eb_begin, eb_end;
+    if (Op::kChunkLoop) {
+        ab = blockIdx.x;
+        eb_begin = 0;
+        eb_end = c.n_eb;
+    } else {
+        ab = blockIdx.x / c.n_eb;
+        eb_begin = blockIdx.x % c.n_eb;
+        eb_end = eb_begin + 1;
+    }
+    const int64_t a0 = ab * c.A_blk;
+    const int tid = threadIdx.x;
+    const int in_shift = ((c.in_shift % L) + L) % L;
+    const int out_shift = ((c.out_shift % L) + L) % L;
+    __syncthreads();
+
+    for (int64_t eb = eb_begin; eb < eb_end; ++eb) {
+        const int64_t e0 = eb * c.E_blk;
+        // ---- step 1: thread (col, t) loads x[t + Q j], j < P --------------------------------
+        {
+            int col, t;
+            if (Op::kLoadLFast) {
+                t = tid % Q;
+                col = tid / Q;
+            } else {
+                col = tid % kCW;
+                t = tid / kCW;
+            }
+            const int al = col / c.E_blk, el = col % c.E_blk;
+            const int64_t a = a0 + al, e = e0 + el;
+            const bool colok = col < c.W && a < c.A && e < c.E;
+            float2 v[P];
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                const int pos = t + Q * j;
+                int l = pos - in_shift;
+                if (l < 0) l += L;
+                v[j] = (colok && l < c.Lin) ? op.load(a, l, e) : make_float2(0.f, 0.f);
+            }
+            if (c.inverse) {
+                dft_reg<P, true>(v, tw, Q);
+#pragma unroll
+                for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<true>(tw, t * k1));
+            } else {
+                dft_reg<P, false>(v, tw, Q);
+#pragma unroll
+                for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<false>(tw, t * k1));
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < P; ++k1) Y[(k1 * Q + t) * CWp + col] = v[k1];
+        }
+        __syncthreads();
+        // ---- step 2: thread (col, k1) runs the Q-point DFT ----------------------------------------
+        const bool s2active = tid < P * kCW;
+        int col2 = 0, k1 = 0;
+        if (Op::kStoreLFast && !Op::kFusedK) {
+            k1 = tid % P;
+            col2 = tid / P;
+        } else {
+            col2 = tid % kCW;
+            k1 = tid / kCW;
+        }
+        const int al2 = col2 / c.E_blk, el2 = col2 % c.E_blk;
+        const int64_t a2 = a0 + al2, e2 = e0 + el2;
+        const bool colok2 = s2active && col2 < c.W && a2 < c.A && e2 < c.E;
+        float2 u[Q];
+        if (s2active) {
+#pragma unroll
+            for (int t = 0; t < Q; ++t) u[t] = Y[(k1 * Q + t) * CWp + col2];
+            if (c.inverse)
+                dft_reg<Q, true>(u, tw, P);
+            else
+                dft_reg<Q, false>(u, tw, P);
+        }
+        if constexpr (Op::kFusedK) {
+            // multiply by the kernel at position k1 + P k2, inverse Q-point DFT over k2
+            __syncthreads();  // everyone has read Y
+            if (s2active) {
+#pragma unroll
+                for (int k2 = 0; k2 < Q; ++k2) u[k2] = colok2 ? cmul(u[k2], op.kval(a2, k1 + P * k2, e2)) : make_float2(0.f, 0.f);
+                if (c.inverse) {
+                    dft_reg<Q, false>(u, tw, P);
+#pragma unroll
+                    for (int n2 = 1; n2 < Q; ++n2) u[n2] = cmul(u[n2], tw_get<false>(tw, n2 * k1));
+                } else {
+                    dft_reg<Q, true>(u, tw, P);
+#pragma unroll
+                    for (int n2 = 1; n2 < Q; ++n2) u[n2] = cmul(u[n2], tw_get<true>(tw, n2 * k1));
+                }
+#pragma unroll
+                for (int n2 = 0; n2 < Q; ++n2) Y[(k1 * Q + n2) * CWp + col2] = u[n2];
+            }
+            __syncthreads();
+            // thread (col, n2): inverse P-point DFT over k1 -> x[n2 + Q n1]
+            {
+                const int col3 = tid % kCW, n2 = tid / kCW;
+                const int al3 = col3 / c.E_blk, el3 = col3 % c.E_blk;
+                const int64_t a3 = a0 + al3, e3 = e0 + el3;
+                const bool colok3 = col3 < c.W && a3 < c.A && e3 < c.E;
+                float2 z[P];
+#pragma unroll
+                for (int q = 0; q < P; ++q) z[q] = Y[(q * Q + n2) * CWp + col3];
+                if (c.inverse)
+                    dft_reg<P, false>(z, tw, Q);
+                else
+                    dft_reg<P, true>(z, tw, Q);
+                if (colok3) {
+#pragma unroll
+                    for (int n1 = 0; n1 < P; ++n1) {
+                        const int pos = n2 + Q * n1;
+                        int o = pos - out_shift;
+                        if (o < 0) o += L;
+                        if (o < c.Lout) op.store(a3, o, e3, z[n1]);
+                    }
+                }
+            }
+        } else if constexpr (Op::kSenseReduce) {
+            // products into Y[o][col], then thread o sums over the columns of its row
+            __syncthreads();  // everyone has read Y
+            if (s2active) {
+#pragma unroll
+                for (int k2 = 0; k2 < Q; ++k2) {
+                    const int pos = k1 + P * k2;
+                    int o = pos - out_shift;
+                    if (o < 0) o += L;
+                    if (o < c.Lout) Y[o * CWp + col2] = colok2 ? op.product(a2, o, e2, u[k2]) : make_float2(0.f, 0.f);
+                }
+            }
+            __syncthreads();
+            const int tot = c.A_blk * c.Lout;
+            for (int idx = tid; idx < tot; idx += blockDim.x) {
+                const int o = idx % c.Lout, al = idx / c.Lout;
+                float2 s = (eb == 0) ? make_float2(0.f, 0.f) : acc[idx];
+                for (int el = 0; el < c.E_blk; ++el) s = cadd(s, Y[o * CWp + al * c.E_blk + el]);
+                acc[idx] = s;
+            }
+        } else {
+            if (colok2) {
+#pragma unroll
+                for (int k2 = 0; k2 < Q; ++k2) {
+                    const int pos = k1 + P * k2;
+                    int o = pos - out_shift;
+                    if (o < 0) o += L;
+                    if (o < c.Lout) op.store(a2, o, e2, u[k2]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if constexpr (Op::kSenseReduce) {
+        const int tot = c.A_blk * c.Lout;
+        for (int idx = tid; idx < tot; idx += blockDim.x) {
+            const int o = idx % c.Lout, al = idx / c.Lout;
+            const int64_t a = a0 + al;
+            if (a < c.A) op.write_row(a, o, acc[idx]);
+        }
+    }
+}
+
+// (P, Q) for the lengths with a register kernel; {0, 0} for the generic kernel.
+inline void reg_split(int L, int* P, int* Q) {
+    switch (L) {
+        case 64: *P = 8; *Q = 8; return;
+        case 128: *P = 8; *Q = 16; return;
+        case 256: *P = 16; *Q = 16; return;
+        case 320: *P = 16; *Q = 20; return;
+        case 512: *P = 16; *Q = 32; return;
+        case 640: *P = 20; *Q = 32; return;
+        default: *P = 0; *Q = 0; return;
+    }
+}
+
+template <int P, int Q, class Op>
+int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s, const char* name) {
+    constexpr int L = P * Q;
+    const size_t smem = (size_t)(L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
+    cudaError_t e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) {
+        set_error(std::string(name) + ": cudaFuncSetAttribute failed: " + cudaGetErrorString(e));
+        return HB_ERR_CUDA;
+    }
+    const int64_t n_ab = ceil_div(c.A, c.A_blk);
+    const int64_t blocks = Op::kChunkLoop ? n_ab : n_ab * c.n_eb;
+    if (blocks <= 0) return HB_OK;
+    if (blocks > 0x7fffffffLL) {
+        set_error(std::string(name) + ": grid too large");
+        return HB_ERR_INVALID_ARG;
+    }
+    TimedSection ts(name, s);
+    pass2_kernel<P, Q, Op><<<(unsigned)blocks, Q * kCW, smem, s>>>(op, c);
+    return check_launch(name);
+}
+
+// Runs the register kernel when L has one, otherwise the generic shared-memory kernel.
+// `extra_per_row` is the kSenseReduce accumulator size per outer row (bytes).
+template <class Op>
+int launch_fft_pass(const Op& op, const FftLen& f, int64_t A, int64_t E, int Lin, int in_shift, int Lout,
+                    int out_shift, int inverse, size_t extra_per_row, cudaStream_t s, const char* name) {
+    int P, Q;
+    reg_split(f.L, &P, &Q);
+    PassCfg c;
+    if (P > 0) {
+        pass_setup(&c, f, A, E, Lin, in_shift, Lout, out_shift, inverse, kCW);
+        const size_t extra = extra_per_row * c.A_blk;
+        switch (f.L) {
+            case 64: return launch_pass2_pq<8, 8>(op, c, extra, s, name);
+            case 128: return launch_pass2_pq<8, 16>(op, c, extra, s, name);
+            case 256: return launch_pass2_pq<16, 16>(op, c, extra, s, name);
+            case 320: return launch_pass2_pq<16, 20>(op, c, extra, s, name);
+            case 512: return launch_pass2_pq<16, 32>(op, c, extra, s, name);
+            case 640: return launch_pass2_pq<20, 32>(op, c, extra, s, name);
+        }
+    }
+    pass_setup(&c, f, A, E, Lin, in_shift, Lout, out_shift, inverse);
+    return launch_pass(op, c, extra_per_row * c.A_blk, s, name);
+}
+
+#endif  // __CUDACC__
+
+}  // namespace hb

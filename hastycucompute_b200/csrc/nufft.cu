@@ -407,11 +407,177 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
     }
 }
 
-// Type-2 interpolation: lanes of a warp map to (point slot, transform); each lane gathers its
-// transform's w^d taps (the CC values of a cell are contiguous), then scatters to the caller's
-// point order.
+// ---- output-stationary spreading ------------------------------------------------------------
+// One CTA owns one tile (one thread per cell) and keeps CC transforms of its cell in registers.
+// Candidate points are staged in shared memory in chunks (first cell relative to the tile, tap
+// weights, CC values); every thread then walks the chunk and accumulates the points whose
+// footprint covers its cell. A warp owns a compact block of cells (2x4x4 in 3-D, 4x8 in 2-D)
+// and skips a point with one vote when the footprint misses the whole block. No atomics except
+// for the extra chunks of dense tiles, which add their partial tile to the grid.
+constexpr int kSpreadChunk = 64;
+
+struct SpreadTileShape {
+    int bz, by, bx;  // warp block
+};
+
 template <int CC>
-__global__ void __launch_bounds__(kGridThreads) k_interp(const GridArgs a) {
+__global__ void __launch_bounds__(512) k_spread_reg(const GridArgs a, int extra_mode, SpreadTileShape wb) {
+    extern __shared__ float sm[];
+    const GridGeom& g = a.g;
+    const int T0 = g.T[0], T1 = g.T[1], T2 = g.T[2];
+    float* coef = sm;                                   // kCoefFloats
+    float* s_w = coef + kCoefFloats;                    // [chunk][3][kMaxWidth]
+    float2* s_val = (float2*)(s_w + kSpreadChunk * 3 * kMaxWidth);  // [chunk][CC]
+    int* s_rel = (int*)(s_val + kSpreadChunk * CC);     // [chunk][3]
+    float* s_sarg = (float*)(s_rel + kSpreadChunk * 3); // [chunk][3]
+    int* s_idx = (int*)(s_sarg + kSpreadChunk * 3);     // [chunk]
+    __shared__ int s_start[8], s_pref[9], s_nbin;
+
+    int tile, chunk;
+    if (extra_mode) {
+        const int2 e = a.extra[blockIdx.x];
+        tile = e.x;
+        chunk = e.y;
+    } else {
+        tile = blockIdx.x;
+        chunk = 0;
+    }
+    const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
+    const int o0 = tz * T0, o1 = ty * T1, o2 = tx * T2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // this thread's cell
+    const int nbx = T2 / wb.bx, nby = T1 / wb.by;
+    const int bxi = warp % nbx, byi = (warp / nbx) % nby, bzi = warp / (nbx * nby);
+    const int cz = bzi * wb.bz + lane / (wb.by * wb.bx);
+    const int cy = byi * wb.by + (lane / wb.bx) % wb.by;
+    const int cx = bxi * wb.bx + lane % wb.bx;
+    const int w0 = g.wa[0], w1 = g.wa[1], w2 = g.wa[2];
+
+    for (int i = tid; i < kCoefFloats; i += blockDim.x) coef[i] = (&a.kb.coef[0][0])[i];
+    if (tid == 0) {
+        int n = 0, acc = 0;
+        for_each_nbr_bin(g.nb, tz, ty, tx, [&](int bin) {
+            const int st = a.bin_start[bin];
+            s_start[n] = st;
+            s_pref[n] = acc;
+            acc += a.bin_start[bin + 1] - st;
+            ++n;
+        });
+        s_pref[n] = acc;
+        s_nbin = n;
+    }
+    __syncthreads();
+    const int total = s_pref[s_nbin];
+    const int k_begin = chunk * a.maxp;
+    const int k_end = min(total, k_begin + a.maxp);
+    const float hw = a.kb.hw;
+
+    for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
+        float ar[CC], ai[CC];
+#pragma unroll
+        for (int c = 0; c < CC; ++c) ar[c] = ai[c] = 0.f;
+        for (int base = k_begin; base < k_end; base += kSpreadChunk) {
+            const int n = min(kSpreadChunk, k_end - base);
+            // stage A: sorted index, first cell relative to the tile, Horner argument
+            if (tid < n) {
+                const int k = base + tid;
+                int b = 0;
+                while (b + 1 < s_nbin && s_pref[b + 1] <= k) ++b;
+                const int s = s_start[b] + (k - s_pref[b]);
+                s_idx[tid] = s;
+                const int org[3] = {o0, o1, o2};
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax) {
+                    if (g.wa[ax] == 1) {
+                        s_rel[tid * 3 + ax] = 0;
+                        s_sarg[tid * 3 + ax] = 0.f;
+                        continue;
+                    }
+                    const float u = a.su[ax][s];
+                    const float v = __fsub_rn(u, hw);
+                    const int ic = (int)ceilf(v);
+                    const float t = __fsub_rn((float)ic, v);
+                    const int nf = g.nf[ax];
+                    int iw = ic;
+                    if (iw < 0) iw += nf;
+                    if (iw >= nf) iw -= nf;
+                    int rel = iw - org[ax];
+                    if (rel < 0) rel += nf;
+                    s_rel[tid * 3 + ax] = rel;
+                    s_sarg[tid * 3 + ax] = fmaf(2.f, t, -1.f);
+                }
+            }
+            __syncthreads();
+            // stage B: tap weights and the CC values of every staged point
+            for (int i = tid; i < n * 3 * kMaxWidth; i += blockDim.x) {
+                const int q = i / (3 * kMaxWidth), r = i % (3 * kMaxWidth), ax = r / kMaxWidth, d = r % kMaxWidth;
+                const int w = g.wa[ax];
+                float val = 0.f;
+                if (d < w) val = (w == 1) ? 1.f : kb_tap(coef, a.kb.deg, d, s_sarg[q * 3 + ax]);
+                s_w[i] = val;
+            }
+            for (int i = tid; i < n * CC; i += blockDim.x) {
+                const int q = i / CC, c = i % CC;
+                s_val[i] = (cc0 + c < g.C) ? a.inT[(int64_t)s_idx[q] * g.C + cc0 + c] : make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+            // accumulate
+            for (int q = 0; q < n; ++q) {
+                int dz = cz - s_rel[q * 3 + 0];
+                int dy = cy - s_rel[q * 3 + 1];
+                int dx = cx - s_rel[q * 3 + 2];
+                if (dz < 0) dz += g.nf[0];
+                if (dy < 0) dy += g.nf[1];
+                if (dx < 0) dx += g.nf[2];
+                const bool in = dz < w0 && dy < w1 && dx < w2;
+                if (__any_sync(0xffffffffu, in)) {
+                    float wgt = 0.f;
+                    if (in)
+                        wgt = s_w[(q * 3 + 0) * kMaxWidth + dz] * s_w[(q * 3 + 1) * kMaxWidth + dy] *
+                              s_w[(q * 3 + 2) * kMaxWidth + dx];
+                    const float2* vq = s_val + q * CC;
+#pragma unroll
+                    for (int c = 0; c < CC; c += 2) {
+                        if (CC == 1) {
+                            const float2 v = vq[0];
+                            ar[0] = fmaf(wgt, v.x, ar[0]);
+                            ai[0] = fmaf(wgt, v.y, ai[0]);
+                        } else {
+                            const float4 v = *reinterpret_cast<const float4*>(vq + c);
+                            ar[c] = fmaf(wgt, v.x, ar[c]);
+                            ai[c] = fmaf(wgt, v.y, ai[c]);
+                            ar[c + 1] = fmaf(wgt, v.z, ar[c + 1]);
+                            ai[c + 1] = fmaf(wgt, v.w, ai[c + 1]);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // write this cell's transforms
+        if (cz < T0 && cy < T1 && cx < T2) {
+            const int64_t gi = ((int64_t)(o0 + cz) * g.nf[1] + (o1 + cy)) * g.nf[2] + (o2 + cx);
+            float2* dst = a.grid + gi * g.C + cc0;
+#pragma unroll
+            for (int c = 0; c < CC; ++c) {
+                if (cc0 + c >= g.C) break;
+                if (extra_mode) {
+                    atomicAdd(&dst[c].x, ar[c]);
+                    atomicAdd(&dst[c].y, ai[c]);
+                } else {
+                    dst[c] = make_float2(ar[c], ai[c]);
+                }
+            }
+        }
+    }
+}
+
+// ---- interpolation with compile-time width ---------------------------------------------------
+// Lanes of a warp map to (point slot, transform). Each lane keeps its point's first cells and tap
+// weights in registers, so the W^d gathers of a point are independent loads the compiler can
+// keep in flight together.
+template <int CC, int W>
+__global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
     extern __shared__ float sm[];
     constexpr int NS = 32 / CC;
     float* coef = sm;
@@ -425,6 +591,7 @@ __global__ void __launch_bounds__(kGridThreads) k_interp(const GridArgs a) {
     const int64_t gwarp = (int64_t)blockIdx.x * kGridWarps + warp;
     const int64_t nwarps = (int64_t)gridDim.x * kGridWarps;
     const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+    const int wz = g.wa[0], wy = g.wa[1];
     for (int64_t base = gwarp * NS; base < g.M; base += nwarps * NS) {
         const int64_t s = base + slot;
         const bool valid = s < g.M;
@@ -432,26 +599,38 @@ __global__ void __launch_bounds__(kGridThreads) k_interp(const GridArgs a) {
         point_setup(a, coef, s, valid, coil, CC, wts, i0);
         __syncwarp();
         if (valid) {
+            int gx[W];
+            float wx[W];
+#pragma unroll
+            for (int d = 0; d < W; ++d) {
+                int v = i0[2] + d;
+                if (v >= nf2) v -= nf2;
+                gx[d] = v;
+                wx[d] = wts[2 * kMaxWidth + d];
+            }
             const int pj = a.perm[s];
             for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
                 if (cc0 + coil >= g.C) break;
+                const float2* gridc = a.grid + cc0 + coil;
                 float ar = 0.f, ai = 0.f;
-                for (int dz = 0; dz < g.wa[0]; ++dz) {
+                for (int dz = 0; dz < wz; ++dz) {
                     int gz = i0[0] + dz;
                     if (gz >= nf0) gz -= nf0;
-                    const float wz = wts[dz];
-                    for (int dy = 0; dy < g.wa[1]; ++dy) {
-                        int gy = i0[1] + dy;
-                        if (gy >= nf1) gy -= nf1;
-                        const float wzy = wz * wts[kMaxWidth + dy];
-                        const int64_t row = ((int64_t)gz * nf1 + gy) * nf2;
-                        for (int dx = 0; dx < g.wa[2]; ++dx) {
-                            int gx = i0[2] + dx;
-                            if (gx >= nf2) gx -= nf2;
-                            const float wgt = wzy * wts[2 * kMaxWidth + dx];
-                            const float2 v = a.grid[(row + gx) * g.C + cc0 + coil];
-                            ar = fmaf(wgt, v.x, ar);
-                            ai = fmaf(wgt, v.y, ai);
+                    const float wzv = wts[dz];
+#pragma unroll
+                    for (int dy = 0; dy < W; ++dy) {
+                        if (dy < wy) {
+                            int gy = i0[1] + dy;
+                            if (gy >= nf1) gy -= nf1;
+                            const float wzy = wzv * wts[kMaxWidth + dy];
+                            const int64_t row = ((int64_t)gz * nf1 + gy) * nf2;
+#pragma unroll
+                            for (int dx = 0; dx < W; ++dx) {
+                                const float2 v = gridc[(row + gx[dx]) * g.C];
+                                const float wgt = wzy * wx[dx];
+                                ar = fmaf(wgt, v.x, ar);
+                                ai = fmaf(wgt, v.y, ai);
+                            }
                         }
                     }
                 }
@@ -466,8 +645,10 @@ __global__ void __launch_bounds__(kGridThreads) k_interp(const GridArgs a) {
 // Load modes f[e][a][l] (a = row over axes 0,1; l = axis 2) pre-scaled by 1/phihat.
 struct OpModesIn {
     static constexpr bool kLoadLFast = true;
+    static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = false;
     static constexpr bool kChunkLoop = false;
+    static constexpr bool kSenseReduce = false;
     const float2* f;
     float2* dst;  // [rows][nf2][C]
     const float* d0;
@@ -480,6 +661,9 @@ struct OpModesIn {
         return cscale(f[e * nm + a * N2 + l], sc);
     }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const { dst[a * d_a + (int64_t)o * d_l + e] = v; }
+    __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
+    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         float2* d = dst;
@@ -492,8 +676,10 @@ struct OpModesIn {
 // Store modes f[e][a][o] scaled by 1/phihat from the interleaved buffer.
 struct OpModesOut {
     static constexpr bool kLoadLFast = false;
+    static constexpr bool kStoreLFast = true;
     static constexpr bool kFusedK = false;
     static constexpr bool kChunkLoop = false;
+    static constexpr bool kSenseReduce = false;
     const float2* src;  // [rows][nf2][C]
     float2* f;
     const float* d0;
@@ -503,12 +689,15 @@ struct OpModesOut {
     int64_t s_a, s_l;
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
+        const float sc = d0[a / N1] * d1[a % N1] * d2[o];
+        f[e * nm + a * N2 + o] = cscale(v, sc);
+    }
+    __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
+    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
-        for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) {
-            const float sc = d0[a / N1] * d1[a % N1] * d2[o];
-            f[e * nm + a * N2 + o] = cscale(v, sc);
-        });
+        for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) { store(a, o, e, v); });
     }
     __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
 };
@@ -772,6 +961,24 @@ template <int CC>
 static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
     const GridGeom& g = p->g;
     const int cells = g.T[0] * g.T[1] * g.T[2];
+    if (cells == 512 && g.dim >= 2) {
+        // output-stationary kernel: one thread per cell of an 8x8x8 (3-D) or 16x32 (2-D) tile
+        SpreadTileShape wb = g.dim == 3 ? SpreadTileShape{2, 4, 4} : SpreadTileShape{1, 4, 8};
+        const size_t smem = sizeof(float) * (kCoefFloats + (size_t)kSpreadChunk * 3 * kMaxWidth) +
+                            sizeof(float2) * (size_t)kSpreadChunk * CC + sizeof(int) * kSpreadChunk * 7;
+        HB_CUDA(cudaFuncSetAttribute(k_spread_reg<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        {
+            TimedSection ts("spread", s);
+            k_spread_reg<CC><<<(unsigned)p->nbins, 512, smem, s>>>(a, 0, wb);
+            HB_TRY(check_launch("k_spread_reg"));
+        }
+        if (p->n_extra > 0) {
+            TimedSection ts("spread_dense", s);
+            k_spread_reg<CC><<<(unsigned)p->n_extra, 512, smem, s>>>(a, 1, wb);
+            HB_TRY(check_launch("k_spread_reg(extra)"));
+        }
+        return HB_OK;
+    }
     const size_t smem = sizeof(float) * ((size_t)2 * cells * CC + kCoefFloats + (size_t)kGridWarps * (32 / CC) * kSlotFloats);
     HB_CUDA(cudaFuncSetAttribute(k_spread<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     {
@@ -787,16 +994,37 @@ static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t 
     return HB_OK;
 }
 
-template <int CC>
-static int launch_interp_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
+template <int CC, int W>
+static int launch_interp_w(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
     const int64_t per_block = (int64_t)kGridWarps * (32 / CC);
     int64_t blocks = ceil_div(std::max<int64_t>(p->g.M, 1), per_block);
     blocks = std::min<int64_t>(blocks, (int64_t)kNumSMs * 64);
     const size_t smem = sizeof(float) * (kCoefFloats + (size_t)kGridWarps * (32 / CC) * kSlotFloats);
-    HB_CUDA(cudaFuncSetAttribute(k_interp<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HB_CUDA(cudaFuncSetAttribute(k_interp_w<CC, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     TimedSection ts("interp", s);
-    k_interp<CC><<<(unsigned)blocks, kGridThreads, smem, s>>>(a);
+    k_interp_w<CC, W><<<(unsigned)blocks, kGridThreads, smem, s>>>(a);
     return check_launch("k_interp");
+}
+
+template <int CC>
+static int launch_interp_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
+    switch (p->kb.w) {
+        case 2: return launch_interp_w<CC, 2>(p, a, s);
+        case 3: return launch_interp_w<CC, 3>(p, a, s);
+        case 4: return launch_interp_w<CC, 4>(p, a, s);
+        case 5: return launch_interp_w<CC, 5>(p, a, s);
+        case 6: return launch_interp_w<CC, 6>(p, a, s);
+        case 7: return launch_interp_w<CC, 7>(p, a, s);
+        case 8: return launch_interp_w<CC, 8>(p, a, s);
+        case 9: return launch_interp_w<CC, 9>(p, a, s);
+        case 10: return launch_interp_w<CC, 10>(p, a, s);
+        case 11: return launch_interp_w<CC, 11>(p, a, s);
+        case 12: return launch_interp_w<CC, 12>(p, a, s);
+        case 13: return launch_interp_w<CC, 13>(p, a, s);
+        case 14: return launch_interp_w<CC, 14>(p, a, s);
+        case 15: return launch_interp_w<CC, 15>(p, a, s);
+        default: return launch_interp_w<CC, 16>(p, a, s);
+    }
 }
 
 static int dispatch_cc(int cc, const NufftPlan* p, const GridArgs& a, cudaStream_t s, bool spread) {
@@ -835,29 +1063,24 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
         float2* other = p->Y;
         // axis 0: [nf0][nf1*nf2*C] -> [Nm0][...]
         if (g.nf[0] > 1) {
-            PassCfg c;
             const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
-            pass_setup(&c, p->fl[0], 1, E, g.nf[0], 0, (int)g.Nm[0], (int)-h0, inv);
             OpStrided op{cur, other, 0, E, 0, E, 1.0f};
-            HB_TRY(launch_pass(op, c, 0, s, "type1 axis0"));
+            HB_TRY(launch_fft_pass(op, p->fl[0], 1, E, g.nf[0], 0, (int)g.Nm[0], (int)-h0, inv, 0, s, "type1 axis0"));
             std::swap(cur, other);
         }
         // axis 1: [Nm0][nf1][nf2*C] -> [Nm0][Nm1][nf2*C]
         if (g.nf[1] > 1) {
-            PassCfg c;
             const int64_t E = (int64_t)g.nf[2] * C;
-            pass_setup(&c, p->fl[1], g.Nm[0], E, g.nf[1], 0, (int)g.Nm[1], (int)-h1, inv);
             OpStrided op{cur, other, (int64_t)g.nf[1] * E, E, g.Nm[1] * E, E, 1.0f};
-            HB_TRY(launch_pass(op, c, 0, s, "type1 axis1"));
+            HB_TRY(launch_fft_pass(op, p->fl[1], g.Nm[0], E, g.nf[1], 0, (int)g.Nm[1], (int)-h1, inv, 0, s, "type1 axis1"));
             std::swap(cur, other);
         }
         // axis 2 -> caller's modes with deapodisation
         {
-            PassCfg c;
-            pass_setup(&c, p->fl[2], g.Nm[0] * g.Nm[1], C, g.nf[2], 0, (int)g.Nm[2], (int)-h2, inv);
             OpModesOut op{cur, out, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm,
                           (int64_t)g.nf[2] * C, C};
-            HB_TRY(launch_pass(op, c, 0, s, "type1 axis2"));
+            HB_TRY(launch_fft_pass(op, p->fl[2], g.Nm[0] * g.Nm[1], C, g.nf[2], 0, (int)g.Nm[2], (int)-h2, inv, 0, s,
+                                   "type1 axis2"));
         }
         return HB_OK;
     }
@@ -867,25 +1090,20 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
     float2* cur = (npass % 2 == 1) ? p->X : p->Y;
     float2* other = (cur == p->X) ? p->Y : p->X;
     {
-        PassCfg c;
-        pass_setup(&c, p->fl[2], g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv);
         OpModesIn op{in, cur, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm, (int64_t)g.nf[2] * C, C};
-        HB_TRY(launch_pass(op, c, 0, s, "type2 axis2"));
+        HB_TRY(launch_fft_pass(op, p->fl[2], g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv, 0, s,
+                               "type2 axis2"));
     }
     if (g.nf[1] > 1) {
-        PassCfg c;
         const int64_t E = (int64_t)g.nf[2] * C;
-        pass_setup(&c, p->fl[1], g.Nm[0], E, (int)g.Nm[1], (int)-h1, g.nf[1], 0, inv);
         OpStrided op{cur, other, g.Nm[1] * E, E, (int64_t)g.nf[1] * E, E, 1.0f};
-        HB_TRY(launch_pass(op, c, 0, s, "type2 axis1"));
+        HB_TRY(launch_fft_pass(op, p->fl[1], g.Nm[0], E, (int)g.Nm[1], (int)-h1, g.nf[1], 0, inv, 0, s, "type2 axis1"));
         std::swap(cur, other);
     }
     if (g.nf[0] > 1) {
-        PassCfg c;
         const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
-        pass_setup(&c, p->fl[0], 1, E, (int)g.Nm[0], (int)-h0, g.nf[0], 0, inv);
         OpStrided op{cur, other, 0, E, 0, E, 1.0f};
-        HB_TRY(launch_pass(op, c, 0, s, "type2 axis0"));
+        HB_TRY(launch_fft_pass(op, p->fl[0], 1, E, (int)g.Nm[0], (int)-h0, g.nf[0], 0, inv, 0, s, "type2 axis0"));
         std::swap(cur, other);
     }
     if (M > 0) {

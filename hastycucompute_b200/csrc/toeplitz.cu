@@ -90,8 +90,10 @@ static int get_len(int L, FftLen* out) {
 
 struct OpToepIn {
     static constexpr bool kLoadLFast = true;
+    static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = false;
     static constexpr bool kChunkLoop = false;
+    static constexpr bool kSenseReduce = false;
     const float2* in;
     const float2* m1;
     const float2* m2;
@@ -106,6 +108,9 @@ struct OpToepIn {
         return v;
     }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const { dst[a * d_a + (int64_t)o * d_l + e] = v; }
+    __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
+    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         float2* d = dst;
@@ -118,14 +123,19 @@ struct OpToepIn {
 // In-place fused pass: FFT, * Kt[col][pos], IFFT, crop. buf[l][e] with row stride E.
 struct OpToepMid {
     static constexpr bool kLoadLFast = false;
+    static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = true;
     static constexpr bool kChunkLoop = false;
+    static constexpr bool kSenseReduce = false;
     float2* buf;
     const float2* kt;
     int64_t E, B;
     int Lk;
     __device__ __forceinline__ float2 load(int64_t, int l, int64_t e) const { return buf[(int64_t)l * E + e]; }
     __device__ __forceinline__ float2 kval(int64_t, int pos, int64_t e) const { return kt[(e / B) * Lk + pos]; }
+    __device__ __forceinline__ void store(int64_t, int o, int64_t e, float2 v) const { buf[(int64_t)o * E + e] = v; }
+    __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
+    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         float2* d = buf;
@@ -137,8 +147,10 @@ struct OpToepMid {
 
 struct OpToepOutFlat {
     static constexpr bool kLoadLFast = false;
+    static constexpr bool kStoreLFast = true;
     static constexpr bool kFusedK = false;
     static constexpr bool kChunkLoop = false;
+    static constexpr bool kSenseReduce = false;
     const float2* src;  // [rows][L2][B]
     int64_t s_a, s_l;
     const float2* in;
@@ -149,17 +161,20 @@ struct OpToepOutFlat {
     int64_t N2, n;
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
+        const int64_t idx = a * N2 + o;
+        if (m1) v = mult_typed(v, m1[idx], out_m1);
+        if (m2) v = mult_typed(v, m2[idx], out_m2);
+        if (io_mult) v = mult_typed(v, in[e * n + idx], io_mult);
+        float2* dst = out + e * n + idx;
+        if (accumulate) v = cadd(v, *dst);
+        *dst = v;
+    }
+    __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
+    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
-        for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) {
-            const int64_t idx = a * N2 + o;
-            if (m1) v = mult_typed(v, m1[idx], out_m1);
-            if (m2) v = mult_typed(v, m2[idx], out_m2);
-            if (io_mult) v = mult_typed(v, in[e * n + idx], io_mult);
-            float2* dst = out + e * n + idx;
-            if (accumulate) v = cadd(v, *dst);
-            *dst = v;
-        });
+        for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) { store(a, o, e, v); });
     }
     __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
 };
@@ -168,8 +183,10 @@ struct OpToepOutFlat {
 // walks every batch chunk of its rows and keeps the running sum in shared memory (extra).
 struct OpToepOutSense {
     static constexpr bool kLoadLFast = false;
+    static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = false;
     static constexpr bool kChunkLoop = true;
+    static constexpr bool kSenseReduce = true;
     const float2* src;
     int64_t s_a, s_l;
     const float2* smaps;
@@ -177,6 +194,11 @@ struct OpToepOutSense {
     int64_t N2, n;
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
+    __device__ __forceinline__ void store(int64_t, int, int64_t, float2) const {}
+    __device__ __forceinline__ float2 product(int64_t a, int o, int64_t e, float2 v) const {
+        return cmulc(v, smaps[e * n + a * N2 + o]);
+    }
+    __device__ __forceinline__ void write_row(int64_t a, int o, float2 v) const { out[a * N2 + o] = v; }
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int Ab, int Eb,
                                                 float2* acc) const {
         const int tot = Ab * c.Lout;
@@ -250,53 +272,42 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
 
     // P1: axis 2, pad N2 -> L2, forward
     {
-        PassCfg c;
-        pass_setup(&c, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0);
         OpToepIn op{a.in, a.m1, a.m2, a.in_m1, a.in_m2, W1, N2, t.n, (int64_t)L2 * B, B};
-        HB_TRY(launch_pass(op, c, 0, s, "toeplitz P1"));
+        HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "toeplitz P1"));
     }
     const int64_t E2 = (int64_t)L2 * B;
     if (t.dim == 3) {
         // P2: axis 1, pad N1 -> L1, forward
         {
-            PassCfg c;
-            pass_setup(&c, f1, N0, E2, (int)N1, 0, L1, 0, 0);
             OpStrided op{W1, W2, N1 * E2, E2, (int64_t)L1 * E2, E2, 1.0f};
-            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P2"));
+            HB_TRY(launch_fft_pass(op, f1, N0, E2, (int)N1, 0, L1, 0, 0, 0, s, "toeplitz P2"));
         }
         // P3: axis 0 fused, in place on W2
         {
-            PassCfg c;
             const int64_t E = (int64_t)L1 * E2;
-            pass_setup(&c, f0, 1, E, (int)N0, 0, (int)N0, (int)(N0 - 1), 0);
             OpToepMid op{W2, a.kt, E, B, L0};
-            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P3"));
+            HB_TRY(launch_fft_pass(op, f0, 1, E, (int)N0, 0, (int)N0, (int)(N0 - 1), 0, 0, s, "toeplitz P3"));
         }
         // P4: axis 1 inverse, crop -> W1
         {
-            PassCfg c;
-            pass_setup(&c, f1, N0, E2, L1, 0, (int)N1, (int)(N1 - 1), 1);
             OpStrided op{W2, W1, (int64_t)L1 * E2, E2, N1 * E2, E2, 1.0f};
-            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P4"));
+            HB_TRY(launch_fft_pass(op, f1, N0, E2, L1, 0, (int)N1, (int)(N1 - 1), 1, 0, s, "toeplitz P4"));
         }
     } else {
         // fused pass along axis 1, in place on W1 ([1][N1][L2][B])
-        PassCfg c;
-        pass_setup(&c, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0);
         OpToepMid op{W1, a.kt, E2, B, L1};
-        HB_TRY(launch_pass(op, c, 0, s, "toeplitz P3"));
+        HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0, 0, s, "toeplitz P3"));
     }
     // P5: axis 2 inverse, crop, output ops
     {
-        PassCfg c;
-        pass_setup(&c, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1);
         if (a.sense) {
             OpToepOutSense op{W1, (int64_t)L2 * B, B, a.in, a.out, N2, t.n};
-            HB_TRY(launch_pass(op, c, sizeof(float2) * (size_t)c.A_blk * c.Lout, s, "toeplitz P5 sense"));
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1, sizeof(float2) * (size_t)N2, s,
+                                   "toeplitz P5 sense"));
         } else {
             OpToepOutFlat op{W1, (int64_t)L2 * B, B, a.in, a.m1, a.m2, a.io_mult, a.out_m1, a.out_m2, a.accumulate,
                              a.out, N2, t.n};
-            HB_TRY(launch_pass(op, c, 0, s, "toeplitz P5"));
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1, 0, s, "toeplitz P5"));
         }
     }
     return HB_OK;
@@ -454,25 +465,22 @@ int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, 
         float2* K = (float2*)kout;
         // axis 2: [r0*r1][r2] -> b1 [r0*r1][L2]
         {
-            PassCfg c;
-            pass_setup(&c, f2, r0 * r1, 1, (int)r2, 0, (int)L[2], 0, 0);
             OpStrided op{red, b1, r2, 1, L[2], 1, 1.0f};
-            if ((st = launch_pass(op, c, 0, s, "toeplitz_kernel axis2")) != HB_OK) break;
+            if ((st = launch_fft_pass(op, f2, r0 * r1, 1, (int)r2, 0, (int)L[2], 0, 0, 0, s, "toeplitz_kernel axis2")) != HB_OK)
+                break;
         }
         // axis 1: [r0][r1][L2] -> [r0][L1][L2]
         {
-            PassCfg c;
-            pass_setup(&c, f1, r0, L[2], (int)r1, 0, (int)L[1], 0, 0);
             float2* dst = dim == 3 ? b2 : K;
             OpStrided op{b1, dst, r1 * L[2], L[2], L[1] * L[2], L[2], dim == 3 ? 1.0f : scale};
-            if ((st = launch_pass(op, c, 0, s, "toeplitz_kernel axis1")) != HB_OK) break;
+            if ((st = launch_fft_pass(op, f1, r0, L[2], (int)r1, 0, (int)L[1], 0, 0, 0, s, "toeplitz_kernel axis1")) != HB_OK)
+                break;
         }
         if (dim == 3) {
-            PassCfg c;
             const int64_t E = L[1] * L[2];
-            pass_setup(&c, f0, 1, E, (int)r0, 0, (int)L[0], 0, 0);
             OpStrided op{b2, K, 0, E, 0, E, scale};
-            if ((st = launch_pass(op, c, 0, s, "toeplitz_kernel axis0")) != HB_OK) break;
+            if ((st = launch_fft_pass(op, f0, 1, E, (int)r0, 0, (int)L[0], 0, 0, 0, s, "toeplitz_kernel axis0")) != HB_OK)
+                break;
         }
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
             set_error(std::string("toeplitz_kernel sync: ") + cudaGetErrorString(e));

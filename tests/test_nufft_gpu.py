@@ -196,3 +196,23 @@ def test_plan_info_matches_oracle_grid(cuda):
         assert info.width == w
         assert abs(info.beta - kb.beta(w)) < 1e-9
         p.free()
+
+
+# Fine grids of 64..640 points run the two-level register FFT kernels; other sizes the generic
+# shared-memory kernel. These cases cover every register length.
+@pytest.mark.gpu
+@pytest.mark.parametrize("nmodes,w", [((32, 32), 4), ((64, 60), 4), ((128, 128), 4), ((160, 150), 6),
+                                      ((256, 250), 4), ((320, 300), 4), ((24, 160), 6)])
+def test_register_fft_lengths(cuda, nmodes, w):
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(sum(nmodes))
+    M, T = 4000, 3
+    coords = rand_coords(rng, 2, M)
+    c = crand(rng, T, M)
+    f = crand(rng, T, *nmodes)
+    p1 = _plan(hb, hb.NufftType.TYPE_1, nmodes, T, w)
+    p1.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p1(to_dev(c, cuda))), gridding.nufft1(coords, c, nmodes, w=w)) <= PARITY
+    p2 = _plan(hb, hb.NufftType.TYPE_2, nmodes, T, w)
+    p2.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p2(to_dev(f, cuda))), gridding.nufft2(coords, f, w=w)) <= PARITY

@@ -121,3 +121,35 @@ def test_workspace_argument(cuda):
         hb.toeplitz_multiplication(to_dev(inp, cuda), out, Kt, small)
     with pytest.raises(hb.HastyError, match="INVALID_ARG"):
         hb.toeplitz_multiplication(to_dev(inp, cuda), out, Kt, None, None, None, 3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,C", [((32, 32, 32), 5), ((64, 64, 64), 2), ((160, 160), 20), ((128, 128), 3),
+                                     ((256, 256), 2), ((320, 320), 1), ((32, 64, 160), 3)])
+def test_register_fft_lengths_sense_and_flat(cuda, shape, C):
+    """2N in {64, 128, 256, 320, 512, 640}: the two-level register FFT kernels."""
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import synthetic
+    rng = np.random.default_rng(C + len(shape))
+    x = crand(rng, *shape)
+    S = synthetic.coil_maps(C, shape)
+    K = crand(rng, *[2 * s for s in shape]).astype(np.complex128)
+    Kd = to_dev(K.astype(np.complex64), cuda)
+    op = hb.NormalTT1Op(Kd, to_dev(S, cuda))
+    assert relerr(to_np(op(to_dev(x, cuda))), otp.sense_normal(x, S, K)) <= PARITY
+    out0 = crand(rng, C, *shape)
+    out = to_dev(out0, cuda)
+    hb.toeplitz_multiplication(to_dev(S, cuda), out, op.kernel_t, None, to_dev(x, cuda), None, 2, 1, 0, 0, 0, 1)
+    ref = otp.toeplitz_multiplication(S, out0, K, x, None, 2, 1, 0, 0, 0, 1)
+    assert relerr(to_np(out), ref) <= PARITY
+
+
+@pytest.mark.gpu
+def test_toeplitz_kernel_register_lengths(cuda):
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(3)
+    shape, M, w = (32, 32, 32), 20000, 6
+    coords = rand_coords(rng, 3, M)
+    K = hb.build_toeplitz_kernel([to_dev(c, cuda) for c in coords], shape, kernel_width=w)
+    ref = otp.toeplitz_kernel(coords, shape, None, w=w)
+    assert relerr(to_np(K), ref) <= PARITY
