@@ -362,6 +362,7 @@ int launch_pass(const Op& op, const PassCfg& c, size_t extra_bytes, cudaStream_t
     const size_t smem = pass_smem_bytes(c, extra_bytes);
     static_assert(kPassThreads == 256, "");
     cudaError_t e = cudaFuncSetAttribute(pass_kernel<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+
     if (e != cudaSuccess) {
         set_error(std::string(name) + ": cudaFuncSetAttribute failed: " + cudaGetErrorString(e));
         return HB_ERR_CUDA;

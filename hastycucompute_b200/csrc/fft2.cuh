@@ -72,6 +72,15 @@ __device__ __forceinline__ void dft_reg(float2* v, const float2* tw, int tws) {
 }
 
 constexpr int kCW = 16;  // columns per CTA
+constexpr int kMaxKCols = 4;  // distinct kernel columns a fused CTA stages in shared memory
+
+// 8-byte asynchronous global -> shared copy (sm_80+ LDGSTS); completes at cp_async_wait_all.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Op contract (in addition to fft.cuh's):
 //   static constexpr bool kStoreLFast    // destination contiguous along the output index
@@ -79,14 +88,20 @@ constexpr int kCW = 16;  // columns per CTA
 //   void store(int64_t a, int o, int64_t e, float2 v) const
 //   float2 product(int64_t a, int o, int64_t e, float2 v) const        (kSenseReduce)
 //   void write_row(int64_t a, int o, float2 v) const                   (kSenseReduce)
+//   int64_t kcol(int64_t e) const; const float2* kptr(int64_t kc) const (kFusedK: column e
+//       multiplies by kptr(kcol(e))[pos]; the CTA stages its distinct columns in shared memory)
+//   const float2* srow(int64_t a, int64_t e) const                      (kSenseReduce: the
+//       factor row of (a, e), staged per chunk; product_s(v, s) combines a value with it)
 template <int P, int Q, class Op>
-__global__ void __launch_bounds__(Q* kCW) pass2_kernel(const Op op, const PassCfg c) {
+__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseReduce || Op::kFusedK) ? 2 : 3)) pass2_kernel(const Op op, const PassCfg c) {
     constexpr int L = P * Q;
     constexpr int CWp = kCW + 1;
     extern __shared__ float2 smem2[];
     float2* tw = smem2;       // L
     float2* Y = smem2 + L;    // [L][CWp] transpose buffer
     float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][Lout] running sums
+    float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * c.Lout : 0);  // kFusedK: [kMaxKCols][L]
+    float2* Ss = Ks + (Op::kFusedK ? kMaxKCols * L : 0);          // kSenseReduce: [W][Lout]
 
     for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = c.tw[i];
 
@@ -108,6 +123,28 @@ __global__ void __launch_bounds__(Q* kCW) pass2_kernel(const Op op, const PassCf
 
     for (int64_t eb = eb_begin; eb < eb_end; ++eb) {
         const int64_t e0 = eb * c.E_blk;
+        // ---- stage the kernel columns / factor rows this chunk needs (asynchronous) -----------
+        int64_t kc0 = 0;
+        bool k_staged = false;
+        if constexpr (Op::kFusedK) {
+            const int64_t elast = min(e0 + c.E_blk, c.E) - 1;
+            kc0 = op.kcol(e0);
+            const int nk = (int)(op.kcol(elast) - kc0 + 1);
+            k_staged = (c.A_blk == 1) && nk <= kMaxKCols;
+            if (k_staged) {
+                for (int i = tid; i < nk * L; i += blockDim.x) cp_async8(Ks + i, op.kptr(kc0 + i / L) + (i % L));
+                cp_async_commit();
+            }
+        }
+        if constexpr (Op::kSenseReduce) {
+            for (int i = tid; i < c.W * c.Lout; i += blockDim.x) {
+                const int col = i / c.Lout, o = i % c.Lout;
+                const int al = col / c.E_blk, el = col % c.E_blk;
+                const int64_t a = a0 + al, e = e0 + el;
+                if (a < c.A && e < c.E) cp_async8(Ss + i, op.srow(a, e) + o);
+            }
+            cp_async_commit();
+        }
         // ---- step 1: thread (col, t) loads x[t + Q j], j < P --------------------------------
         {
             int col, t;
@@ -141,6 +178,7 @@ __global__ void __launch_bounds__(Q* kCW) pass2_kernel(const Op op, const PassCf
 #pragma unroll
             for (int k1 = 0; k1 < P; ++k1) Y[(k1 * Q + t) * CWp + col] = v[k1];
         }
+        if (Op::kFusedK || Op::kSenseReduce) cp_async_wait_all();
         __syncthreads();
         // ---- step 2: thread (col, k1) runs the Q-point DFT ----------------------------------------
         const bool s2active = tid < P * kCW;
@@ -169,7 +207,14 @@ __global__ void __launch_bounds__(Q* kCW) pass2_kernel(const Op op, const PassCf
             __syncthreads();  // everyone has read Y
             if (s2active) {
 #pragma unroll
-                for (int k2 = 0; k2 < Q; ++k2) u[k2] = colok2 ? cmul(u[k2], op.kval(a2, k1 + P * k2, e2)) : make_float2(0.f, 0.f);
+                if (k_staged) {
+                    const float2* kc = Ks + (int)(op.kcol(e2) - kc0) * L;
+#pragma unroll
+                    for (int k2 = 0; k2 < Q; ++k2) u[k2] = colok2 ? cmul(u[k2], kc[k1 + P * k2]) : make_float2(0.f, 0.f);
+                } else {
+#pragma unroll
+                    for (int k2 = 0; k2 < Q; ++k2) u[k2] = colok2 ? cmul(u[k2], op.kval(a2, k1 + P * k2, e2)) : make_float2(0.f, 0.f);
+                }
                 if (c.inverse) {
                     dft_reg<Q, false>(u, tw, P);
 #pragma unroll
@@ -207,7 +252,7 @@ __global__ void __launch_bounds__(Q* kCW) pass2_kernel(const Op op, const PassCf
                 }
             }
         } else if constexpr (Op::kSenseReduce) {
-            // products into Y[o][col], then thread o sums over the columns of its row
+            // spectra into Y[o][col]; then thread o forms sum_col product(v) for its row
             __syncthreads();  // everyone has read Y
             if (s2active) {
 #pragma unroll
@@ -215,16 +260,24 @@ __global__ void __launch_bounds__(Q* kCW) pass2_kernel(const Op op, const PassCf
                     const int pos = k1 + P * k2;
                     int o = pos - out_shift;
                     if (o < 0) o += L;
-                    if (o < c.Lout) Y[o * CWp + col2] = colok2 ? op.product(a2, o, e2, u[k2]) : make_float2(0.f, 0.f);
+                    if (o < c.Lout) Y[o * CWp + col2] = u[k2];
                 }
             }
             __syncthreads();
             const int tot = c.A_blk * c.Lout;
             for (int idx = tid; idx < tot; idx += blockDim.x) {
                 const int o = idx % c.Lout, al = idx / c.Lout;
-                float2 s = (eb == 0) ? make_float2(0.f, 0.f) : acc[idx];
-                for (int el = 0; el < c.E_blk; ++el) s = cadd(s, Y[o * CWp + al * c.E_blk + el]);
-                acc[idx] = s;
+                const int64_t a = a0 + al;
+                float2 sum = (eb == 0) ? make_float2(0.f, 0.f) : acc[idx];
+                if (a < c.A) {
+                    for (int el = 0; el < c.E_blk; ++el) {
+                        const int64_t e = e0 + el;
+                        if (e >= c.E) break;
+                        const int col = al * c.E_blk + el;
+                        sum = cadd(sum, op.product_s(Y[o * CWp + col], Ss[col * c.Lout + o]));
+                    }
+                }
+                acc[idx] = sum;
             }
         } else {
             if (colok2) {
@@ -265,8 +318,14 @@ inline void reg_split(int L, int* P, int* Q) {
 template <int P, int Q, class Op>
 int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s, const char* name) {
     constexpr int L = P * Q;
-    const size_t smem = (size_t)(L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
+    size_t smem = (size_t)(L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
+    if (Op::kFusedK) smem += (size_t)kMaxKCols * L * sizeof(float2);
+    if (Op::kSenseReduce) smem += (size_t)c.W * c.Lout * sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the staging passes want every CTA they can fit; plain passes keep the default L1 split
+    if (e == cudaSuccess && (Op::kFusedK || Op::kSenseReduce))
+        e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) {
         set_error(std::string(name) + ": cudaFuncSetAttribute failed: " + cudaGetErrorString(e));
         return HB_ERR_CUDA;

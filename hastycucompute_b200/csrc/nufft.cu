@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
 // footprint covers its cell. A warp owns a compact block of cells (2x4x4 in 3-D, 4x8 in 2-D)
 // and skips a point with one vote when the footprint misses the whole block. No atomics except
 // for the extra chunks of dense tiles, which add their partial tile to the grid.
-constexpr int kSpreadChunk = 64;
+constexpr int kSpreadChunk = 128;
 
 struct SpreadTileShape {
     int bz, by, bx;  // warp block
@@ -431,6 +431,7 @@ __global__ void __launch_bounds__(512) k_spread_reg(const GridArgs a, int extra_
     int* s_rel = (int*)(s_val + kSpreadChunk * CC);     // [chunk][3]
     float* s_sarg = (float*)(s_rel + kSpreadChunk * 3); // [chunk][3]
     int* s_idx = (int*)(s_sarg + kSpreadChunk * 3);     // [chunk]
+    unsigned* s_mask = (unsigned*)(s_idx + kSpreadChunk); // [chunk] warps whose block the footprint meets
     __shared__ int s_start[8], s_pref[9], s_nbin;
 
     int tile, chunk;
@@ -506,6 +507,31 @@ __global__ void __launch_bounds__(512) k_spread_reg(const GridArgs a, int extra_
                     s_rel[tid * 3 + ax] = rel;
                     s_sarg[tid * 3 + ax] = fmaf(2.f, t, -1.f);
                 }
+                // which warp blocks the footprint meets, per axis, then combined
+                const int bsz[3] = {wb.bz, wb.by, wb.bx};
+                const int nblk[3] = {T0 / wb.bz, T1 / wb.by, T2 / wb.bx};
+                unsigned am[3];
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax) {
+                    am[ax] = 0u;
+                    const int rel = s_rel[tid * 3 + ax], w = g.wa[ax], nf = g.nf[ax];
+                    for (int bi = 0; bi < nblk[ax]; ++bi)
+                        for (int cc = bi * bsz[ax]; cc < (bi + 1) * bsz[ax]; ++cc) {
+                            int d = cc - rel;
+                            if (d < 0) d += nf;
+                            if (d < w) {
+                                am[ax] |= 1u << bi;
+                                break;
+                            }
+                        }
+                }
+                unsigned m = 0u;
+                const int nw = nblk[0] * nblk[1] * nblk[2];
+                for (int wi = 0; wi < nw; ++wi) {
+                    const int xi = wi % nblk[2], yi = (wi / nblk[2]) % nblk[1], zi = wi / (nblk[2] * nblk[1]);
+                    if (((am[0] >> zi) & (am[1] >> yi) & (am[2] >> xi) & 1u) != 0u) m |= 1u << wi;
+                }
+                s_mask[tid] = m;
             }
             __syncthreads();
             // stage B: tap weights and the CC values of every staged point
@@ -521,16 +547,21 @@ __global__ void __launch_bounds__(512) k_spread_reg(const GridArgs a, int extra_
                 s_val[i] = (cc0 + c < g.C) ? a.inT[(int64_t)s_idx[q] * g.C + cc0 + c] : make_float2(0.f, 0.f);
             }
             __syncthreads();
-            // accumulate
-            for (int q = 0; q < n; ++q) {
-                int dz = cz - s_rel[q * 3 + 0];
-                int dy = cy - s_rel[q * 3 + 1];
-                int dx = cx - s_rel[q * 3 + 2];
-                if (dz < 0) dz += g.nf[0];
-                if (dy < 0) dy += g.nf[1];
-                if (dx < 0) dx += g.nf[2];
-                const bool in = dz < w0 && dy < w1 && dx < w2;
-                if (__any_sync(0xffffffffu, in)) {
+            // accumulate: each warp visits only the staged points whose footprint meets its block
+            for (int q0 = 0; q0 < n; q0 += 32) {
+                const int qq = q0 + lane;
+                const bool hit = qq < n && ((s_mask[qq] >> warp) & 1u);
+                unsigned bits = __ballot_sync(0xffffffffu, hit);
+                while (bits) {
+                    const int q = q0 + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    int dz = cz - s_rel[q * 3 + 0];
+                    int dy = cy - s_rel[q * 3 + 1];
+                    int dx = cx - s_rel[q * 3 + 2];
+                    if (dz < 0) dz += g.nf[0];
+                    if (dy < 0) dy += g.nf[1];
+                    if (dx < 0) dx += g.nf[2];
+                    const bool in = dz < w0 && dy < w1 && dx < w2;
                     float wgt = 0.f;
                     if (in)
                         wgt = s_w[(q * 3 + 0) * kMaxWidth + dz] * s_w[(q * 3 + 1) * kMaxWidth + dy] *
@@ -599,16 +630,19 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
         point_setup(a, coef, s, valid, coil, CC, wts, i0);
         __syncwarp();
         if (valid) {
-            int gx[W];
+            // element offsets of the taps along axis 2 (x C transforms), 32-bit: a grid holds
+            // fewer than 2^32 complex values (checked when the plan is made)
+            unsigned colofs[W];
             float wx[W];
 #pragma unroll
             for (int d = 0; d < W; ++d) {
                 int v = i0[2] + d;
                 if (v >= nf2) v -= nf2;
-                gx[d] = v;
+                colofs[d] = (unsigned)v * (unsigned)g.C;
                 wx[d] = wts[2 * kMaxWidth + d];
             }
             const int pj = a.perm[s];
+            const unsigned rowstride = (unsigned)nf2 * (unsigned)g.C;
             for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
                 if (cc0 + coil >= g.C) break;
                 const float2* gridc = a.grid + cc0 + coil;
@@ -623,10 +657,10 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
                             int gy = i0[1] + dy;
                             if (gy >= nf1) gy -= nf1;
                             const float wzy = wzv * wts[kMaxWidth + dy];
-                            const int64_t row = ((int64_t)gz * nf1 + gy) * nf2;
+                            const unsigned rowbase = ((unsigned)gz * (unsigned)nf1 + (unsigned)gy) * rowstride;
 #pragma unroll
                             for (int dx = 0; dx < W; ++dx) {
-                                const float2 v = gridc[(row + gx[dx]) * g.C];
+                                const float2 v = gridc[rowbase + colofs[dx]];
                                 const float wgt = wzy * wx[dx];
                                 ar = fmaf(wgt, v.x, ar);
                                 ai = fmaf(wgt, v.y, ai);
@@ -660,6 +694,10 @@ struct OpModesIn {
         const float sc = d0[a / N1] * d1[a % N1] * d2[l];
         return cscale(f[e * nm + a * N2 + l], sc);
     }
+    __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
+    __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
+    __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
+    __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const { dst[a * d_a + (int64_t)o * d_l + e] = v; }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
@@ -688,6 +726,10 @@ struct OpModesOut {
     int64_t N1, N2, nm;
     int64_t s_a, s_l;
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
+    __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
+    __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
+    __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
+    __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
         const float sc = d0[a / N1] * d1[a % N1] * d2[o];
@@ -794,6 +836,8 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
         HB_CUDA(cudaMemcpy(p->deapod[ax], dv.data(), sizeof(float) * dv.size(), cudaMemcpyHostToDevice));
     }
     p->X_elems = (size_t)g.nf[0] * g.nf[1] * g.nf[2] * g.C;
+    HB_REQUIRE(p->X_elems < ((size_t)1 << 32), HB_ERR_INVALID_ARG,
+               "fine grid x ntransf must hold fewer than 2^32 values; split the transforms");
     p->Y_elems = (size_t)g.Nm[0] * g.nf[1] * g.nf[2] * g.C;
     HB_TRY(dev_alloc(p, (void**)&p->X, sizeof(float2) * p->X_elems, "fine grid"));
     HB_TRY(dev_alloc(p, (void**)&p->Y, sizeof(float2) * p->Y_elems, "pass buffer"));
@@ -965,7 +1009,7 @@ static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t 
         // output-stationary kernel: one thread per cell of an 8x8x8 (3-D) or 16x32 (2-D) tile
         SpreadTileShape wb = g.dim == 3 ? SpreadTileShape{2, 4, 4} : SpreadTileShape{1, 4, 8};
         const size_t smem = sizeof(float) * (kCoefFloats + (size_t)kSpreadChunk * 3 * kMaxWidth) +
-                            sizeof(float2) * (size_t)kSpreadChunk * CC + sizeof(int) * kSpreadChunk * 7;
+                            sizeof(float2) * (size_t)kSpreadChunk * CC + sizeof(int) * kSpreadChunk * 8;
         HB_CUDA(cudaFuncSetAttribute(k_spread_reg<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         {
             TimedSection ts("spread", s);

@@ -22,6 +22,10 @@ struct OpStrided {
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
         return src[a * s_a + (int64_t)l * s_l + e];
     }
+    __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
+    __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
+    __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
+    __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
         dst[a * d_a + (int64_t)o * d_l + e] = cscale(v, scale);

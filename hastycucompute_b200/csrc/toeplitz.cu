@@ -107,6 +107,10 @@ struct OpToepIn {
         if (m2) v = mult_typed(v, m2[idx], in_m2);
         return v;
     }
+    __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
+    __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
+    __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
+    __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const { dst[a * d_a + (int64_t)o * d_l + e] = v; }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
@@ -132,6 +136,10 @@ struct OpToepMid {
     int64_t E, B;
     int Lk;
     __device__ __forceinline__ float2 load(int64_t, int l, int64_t e) const { return buf[(int64_t)l * E + e]; }
+    __device__ __forceinline__ int64_t kcol(int64_t e) const { return e / B; }
+    __device__ __forceinline__ const float2* kptr(int64_t kc) const { return kt + kc * Lk; }
+    __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
+    __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
     __device__ __forceinline__ float2 kval(int64_t, int pos, int64_t e) const { return kt[(e / B) * Lk + pos]; }
     __device__ __forceinline__ void store(int64_t, int o, int64_t e, float2 v) const { buf[(int64_t)o * E + e] = v; }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
@@ -160,6 +168,10 @@ struct OpToepOutFlat {
     float2* out;
     int64_t N2, n;
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
+    __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
+    __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
+    __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
+    __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
         const int64_t idx = a * N2 + o;
@@ -193,6 +205,10 @@ struct OpToepOutSense {
     float2* out;
     int64_t N2, n;
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
+    __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
+    __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
+    __device__ __forceinline__ const float2* srow(int64_t a, int64_t e) const { return smaps + e * n + a * N2; }
+    __device__ __forceinline__ float2 product_s(float2 v, float2 sv) const { return cmulc(v, sv); }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t, int, int64_t, float2) const {}
     __device__ __forceinline__ float2 product(int64_t a, int o, int64_t e, float2 v) const {
@@ -492,3 +508,4 @@ int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, 
 }
 
 }  // namespace hb
+
