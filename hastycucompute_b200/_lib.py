@@ -41,6 +41,7 @@ SIGNATURES = {
     "hb_toeplitz_multiplication": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _sz, _vp, _vp,
                                         _i, _i, _i, _i, _i, _i, _vp]),
     "hb_sense_normal": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "hb_sense_normal_noalloc": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp]),
     "hb_cg_state_bytes": (_sz, []),
     "hb_cg_init": (_i, [_i64, _vp, _vp, _vp, _vp, _vp, _d, _vp]),
     "hb_cg_step": (_i, [_i64, _vp, _vp, _vp, _vp, _vp, _vp]),

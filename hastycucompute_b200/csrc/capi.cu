@@ -23,6 +23,8 @@ int toeplitz_multiplication(int dim, const int64_t* shape, int64_t nbatch, const
                             cudaStream_t s);
 int sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps, const void* kernel,
                  void* out, void* workspace, size_t workspace_bytes, cudaStream_t s);
+int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps,
+                         const void* kernel, void* out, cudaStream_t s);
 size_t cg_state_bytes();
 int cg_init(int64_t n, const void* b, const void* Ax, void* r, void* p, void* state, double tol, cudaStream_t s);
 int cg_step(int64_t n, void* x, void* r, void* p, const void* Ap, void* state, cudaStream_t s);
@@ -158,6 +160,11 @@ int hb_sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x
         return hb::sense_normal(dim, shape, ncoils, x, smaps, kernel, out, workspace, workspace_bytes,
                                 as_stream(stream));
     })
+}
+
+int hb_sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps,
+                            const void* kernel, void* out, void* stream) {
+    HB_GUARD({ return hb::sense_normal_noalloc(dim, shape, ncoils, x, smaps, kernel, out, as_stream(stream)); })
 }
 
 size_t hb_cg_state_bytes(void) { return hb::cg_state_bytes(); }

@@ -12,6 +12,7 @@
 // A 2-D apply is P1, the fused pass along axis 1, and P5.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "nufft.cuh"
@@ -509,3 +510,126 @@ int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, 
 
 }  // namespace hb
 
+// ---- allocation-free SENSE normal operator ------------------------------------------------------
+// For callers that cannot allocate device memory: an allocator-less runtime embedded in another
+// framework, a driver layer that hands out only fixed buffers, or code running where
+// cudaMalloc is off limits. The workspace and the FFT twiddle tables live in file-scope device
+// arrays of fixed size that every GPU loading this library keeps until the process exits.
+namespace hb {
+
+constexpr size_t kNoAllocWsBytes = size_t(32) << 20;  // 32 MiB of workspace
+constexpr int kNoAllocMaxLen = 4096;                  // longest 2N per axis
+static __device__ __align__(256) float2 g_noalloc_ws[kNoAllocWsBytes / sizeof(float2)];
+static __device__ __align__(256) float2 g_noalloc_tw[3 * kNoAllocMaxLen];
+
+struct NoAllocDevice {
+    float2* ws = nullptr;
+    float2* tw = nullptr;
+};
+static std::mutex g_noalloc_mu;
+static std::vector<NoAllocDevice> g_noalloc_dev;
+
+// Device addresses of the two arrays for the current device, looked up once per device.
+static int noalloc_addresses(NoAllocDevice* out) {
+    int dev = 0;
+    HB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if ((int)g_noalloc_dev.size() <= dev) g_noalloc_dev.resize(dev + 1);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (d.ws == nullptr || d.tw == nullptr) {
+        void* ws = nullptr;
+        void* tw = nullptr;
+        HB_CUDA(cudaGetSymbolAddress(&ws, g_noalloc_ws));
+        HB_CUDA(cudaGetSymbolAddress(&tw, g_noalloc_tw));
+        d.ws = (float2*)ws;
+        d.tw = (float2*)tw;
+    }
+    *out = d;
+    return HB_OK;
+}
+
+__global__ void k_fill_twiddles(float2* tw, int L) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= L) return;
+    double sn, cs;
+    sincospi(-2.0 * (double)m / (double)L, &sn, &cs);
+    tw[m] = make_float2((float)cs, (float)sn);
+}
+
+// Radix plan of L (same factor order as fftlen_make) with the twiddles at `tw`.
+static int noalloc_len(int L, float2* tw, cudaStream_t s, FftLen* f) {
+    f->L = L;
+    f->nrad = 0;
+    f->tw = tw;
+    int rest = L;
+    for (int r : {8, 4, 2, 5, 3, 7}) {
+        while (rest % r == 0 && rest > 1) {
+            HB_REQUIRE(f->nrad < kMaxRadices, HB_ERR_INVALID_ARG, "FFT length has too many factors");
+            f->rad[f->nrad++] = r;
+            rest /= r;
+        }
+    }
+    HB_REQUIRE(rest == 1, HB_ERR_INVALID_ARG, "2N must be 2,3,5,7-smooth on every axis");
+    k_fill_twiddles<<<(unsigned)ceil_div(L, 256), 256, 0, s>>>(tw, L);
+    return check_launch("k_fill_twiddles");
+}
+
+int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps,
+                         const void* kernel, void* out, cudaStream_t s) {
+    ToepGeom t;
+    HB_TRY(toep_geom(&t, dim, shape, ncoils));
+    HB_REQUIRE(x && smaps && kernel && out, HB_ERR_INVALID_ARG, "x, smaps, kernel and out must be non-null");
+    HB_REQUIRE(out != x, HB_ERR_INVALID_ARG, "out must not alias x");
+    const size_t need = toep_ws_elems(t) * sizeof(float2);
+    if (need > kNoAllocWsBytes) {
+        set_error("hb_sense_normal_noalloc: problem needs " + std::to_string(need) +
+                  " bytes of workspace, the fixed array holds " + std::to_string(kNoAllocWsBytes) +
+                  " (6 * prod(N) * ncoils * 8 bytes must fit)");
+        return HB_ERR_WORKSPACE;
+    }
+    for (int ax = 0; ax < 3; ++ax)
+        HB_REQUIRE(t.L[ax] <= kNoAllocMaxLen, HB_ERR_INVALID_ARG, "hb_sense_normal_noalloc: 2N must be <= 4096");
+    NoAllocDevice d;
+    HB_TRY(noalloc_addresses(&d));
+    FftLen f0, f1, f2;
+    HB_TRY(noalloc_len(t.L[2], d.tw + 2 * kNoAllocMaxLen, s, &f2));
+    HB_TRY(noalloc_len(t.L[1], d.tw + 1 * kNoAllocMaxLen, s, &f1));
+    if (t.dim == 3) HB_TRY(noalloc_len(t.L[0], d.tw, s, &f0));
+
+    const int64_t B = t.B, N0 = t.N[0], N1 = t.N[1], N2 = t.N[2];
+    const int L0 = t.L[0], L1 = t.L[1], L2 = t.L[2];
+    const float2* S = (const float2*)smaps;
+    float2* W1 = d.ws;
+    float2* W2 = d.ws + (size_t)N0 * N1 * L2 * B;
+    const int64_t E2 = (int64_t)L2 * B;
+    {
+        OpToepIn op{S, (const float2*)x, nullptr, HB_MULT_MULT, HB_MULT_NONE, W1, N2, t.n, E2, B};
+        HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "noalloc P1"));
+    }
+    if (t.dim == 3) {
+        {
+            OpStrided op{W1, W2, N1 * E2, E2, (int64_t)L1 * E2, E2, 1.0f};
+            HB_TRY(launch_fft_pass(op, f1, N0, E2, (int)N1, 0, L1, 0, 0, 0, s, "noalloc P2"));
+        }
+        {
+            const int64_t E = (int64_t)L1 * E2;
+            OpToepMid op{W2, (const float2*)kernel, E, B, L0};
+            HB_TRY(launch_fft_pass(op, f0, 1, E, (int)N0, 0, (int)N0, (int)(N0 - 1), 0, 0, s, "noalloc P3"));
+        }
+        {
+            OpStrided op{W2, W1, (int64_t)L1 * E2, E2, N1 * E2, E2, 1.0f};
+            HB_TRY(launch_fft_pass(op, f1, N0, E2, L1, 0, (int)N1, (int)(N1 - 1), 1, 0, s, "noalloc P4"));
+        }
+    } else {
+        OpToepMid op{W1, (const float2*)kernel, E2, B, L1};
+        HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0, 0, s, "noalloc P3"));
+    }
+    {
+        OpToepOutSense op{W1, E2, B, S, (float2*)out, N2, t.n};
+        HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1, sizeof(float2) * (size_t)N2, s,
+                               "noalloc P5 sense"));
+    }
+    return HB_OK;
+}
+
+}  // namespace hb

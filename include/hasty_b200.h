@@ -151,6 +151,19 @@ int hb_sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x
                     const void* smaps, const void* kernel, void* out,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of hb_sense_normal (no counterpart in the reference). For callers
+ * that cannot allocate device memory -- a runtime embedded in another framework that owns all
+ * allocations, a driver layer handing out fixed buffers, code running where cudaMalloc is off
+ * limits. It allocates nothing: the workspace (32 MiB) and the FFT twiddle tables sit in fixed
+ * device arrays inside this library, which every GPU that loads it keeps until exit. Limits:
+ * 6 * prod(N) * ncoils * 8 bytes <= 32 MiB (else HB_ERR_WORKSPACE, nothing launched) and
+ * 2N <= 4096 per axis. The first call on a device looks up the arrays' device addresses; make
+ * that first call before any stream capture. All calls share the arrays, so calls that overlap
+ * on the GPU (different streams, threads or processes sharing a context) race: serialise them.
+ * Result as hb_sense_normal. */
+int hb_sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x,
+                            const void* smaps, const void* kernel, void* out, void* stream);
+
 /* ---- conjugate gradient --------------------------------------------------------------
  * Vector steps of conjugate_gradient, cpp/corelib/lib/op/cg.cppm:122-184, with all scalars
  * on the device (no host read per iteration) and every inner product accumulated in FP64
