@@ -4,7 +4,17 @@ NUFFT type 1 / 2 (``nufft``), the Toeplitz-embedded normal operator and SENSE A^
 (``toeplitz``, ``normal``) and conjugate gradient (``cg``), over the C ABI of libhasty_b200.so.
 """
 from ._lib import HastyError, load as load_library  # noqa: F401
-from .nufft import NufftMethod, NufftOpts, NufftPlan, NufftSign, NufftType, NufftUpsamp  # noqa: F401
+from .nufft import (  # noqa: F401
+    NufftMethod,
+    NufftOpts,
+    NufftPlan,
+    NufftSign,
+    NufftType,
+    NufftUpsamp,
+    nufft_backward_cpu_over_cuda,
+    nufft_type1,
+    nufft_type2,
+)
 from .toeplitz import (  # noqa: F401
     ToeplitzAccumulateType,
     ToeplitzMultType,
@@ -14,7 +24,16 @@ from .toeplitz import (  # noqa: F401
     toeplitz_multiply,
     transform_toeplitz_kernel,
 )
-from .normal import NormalTT1Op, SenseOp, build_toeplitz_kernel  # noqa: F401
-from .cg import CGSolver, conjugate_gradient, vdot_real  # noqa: F401
+from .normal import (  # noqa: F401
+    BatchedNormalOp,
+    NormalTT1Op,
+    NormalTT2Op,
+    SenseOffresOp,
+    SenseOp,
+    build_toeplitz_kernel,
+    build_toeplitz_kernels,
+)
+from .cg import BatchedCGSolver, CGSolver, conjugate_gradient, vdot_real  # noqa: F401
+from . import autograd  # noqa: F401
 
 __version__ = "0.1.0"

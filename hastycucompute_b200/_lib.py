@@ -34,6 +34,8 @@ SIGNATURES = {
     "hb_nufft_setpts": (_i, [_vp, _i64, _vp, _vp, _vp, _vp]),
     "hb_nufft_execute": (_i, [_vp, _vp, _vp, _vp]),
     "hb_nufft_destroy": (_i, [_vp]),
+    "hb_nufft_coord_grad": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "hb_nufft_set_spread_tuning": (_i, [_vp, _i, _i, _i, _i]),
     "hb_nufft_get_info": (_i, [_vp, _pi64, C.POINTER(_i), C.POINTER(_d), C.POINTER(_sz)]),
     "hb_toeplitz_kernel": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "hb_transform_toeplitz_kernel": (_i, [_i, _pi64, _vp, _vp, _vp]),
@@ -42,6 +44,12 @@ SIGNATURES = {
                                         _i, _i, _i, _i, _i, _i, _vp]),
     "hb_sense_normal": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hb_sense_normal_noalloc": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "hb_sense_normal_batched": (_i, [_i, _pi64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "hb_transform_toeplitz_kernels": (_i, [_i, _pi64, _i64, _vp, _vp, _vp]),
+    "hb_cgb_state_bytes": (_sz, [_i64]),
+    "hb_cgb_init": (_i, [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _d, _vp]),
+    "hb_cgb_step": (_i, [_i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hb_cgb_read_state": (_i, [_vp, _i64, C.POINTER(_d), _pi64, C.POINTER(_i), _vp]),
     "hb_cg_state_bytes": (_sz, []),
     "hb_cg_init": (_i, [_i64, _vp, _vp, _vp, _vp, _vp, _d, _vp]),
     "hb_cg_step": (_i, [_i64, _vp, _vp, _vp, _vp, _vp, _vp]),

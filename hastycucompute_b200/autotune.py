@@ -1,0 +1,107 @@
+"""Spreading autotuner: picks the warp cell-block shape and the points per spread subproblem for a
+given problem by timing type-1 plans on the device, and caches the choice as JSON.
+
+Search space (all exact, all give the same result up to float rounding):
+- the 32-cell block each warp owns inside a spread tile: 3-D tiles are 8x8x8, so any
+  (bz, by, bx) with bz*by*bx = 32 and each edge dividing 8; 2-D tiles are 16x32;
+- points per subproblem (how dense tiles are split across CTAs): 512 .. 4096.
+
+Cache key: dimensionality, modes, transforms, kernel width, number of points and a coarse
+density signature of the trajectory (quartiles of |k|), so the same trajectory family reuses the
+choice. Cache file: $HASTY_B200_TUNE_CACHE or ~/.cache/hastycucompute_b200/spread_tuning.json.
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+from typing import Optional, Sequence
+
+import torch
+
+from .nufft import NufftOpts, NufftPlan, NufftType
+
+BLOCKS_3D = [(2, 4, 4), (4, 4, 2), (2, 2, 8), (4, 2, 4), (1, 4, 8), (8, 2, 2), (2, 8, 2)]
+BLOCKS_2D = [(1, 4, 8), (1, 8, 4), (1, 2, 16), (1, 16, 2), (1, 1, 32)]
+MAXP = [512, 1024, 2048, 4096]
+
+
+def cache_path() -> Path:
+    p = os.environ.get("HASTY_B200_TUNE_CACHE")
+    if p:
+        return Path(p)
+    return Path.home() / ".cache" / "hastycucompute_b200" / "spread_tuning.json"
+
+
+def _key(nmodes, ntransf, width, coords) -> str:
+    r = torch.sqrt(sum(c.float() ** 2 for c in coords))
+    q = torch.quantile(r[:: max(1, r.numel() // 100000)], torch.tensor([0.25, 0.5, 0.75], device=r.device))
+    sig = ",".join(f"{v:.2f}" for v in q.tolist())
+    M = coords[0].shape[0]
+    return f"d{len(nmodes)}|n{'x'.join(map(str, nmodes))}|t{ntransf}|w{width}|m{M // 1000}k|q{sig}"
+
+
+def _load() -> dict:
+    p = cache_path()
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+def _store(d: dict) -> None:
+    p = cache_path()
+    p.parent.mkdir(parents=True, exist_ok=True)
+    p.write_text(json.dumps(d, indent=1, sort_keys=True))
+
+
+def tune_spread(nmodes: Sequence[int], ntransf: int, coords: Sequence[torch.Tensor], kernel_width: int,
+                reps: int = 3, use_cache: bool = True, candidates: Optional[list] = None) -> dict:
+    """Times type-1 executes over the search space; returns {"block", "max_candidates", "ms",
+    "timings"} for the fastest and stores it in the cache."""
+    nmodes = tuple(int(n) for n in nmodes)
+    key = _key(nmodes, ntransf, kernel_width, coords)
+    cache = _load() if use_cache else {}
+    if key in cache:
+        return dict(cache[key], cached=True)
+    dev = coords[0].device
+    blocks = BLOCKS_3D if len(nmodes) == 3 else BLOCKS_2D
+    if candidates is None:
+        candidates = [(b, m) for b in blocks for m in MAXP]
+    M = coords[0].shape[0]
+    data = torch.randn((ntransf, M), dtype=torch.complex64, device=dev)
+    out = torch.empty((ntransf, *nmodes), dtype=torch.complex64, device=dev)
+    timings = []
+    for block, maxp in candidates:
+        plan = NufftPlan(NufftType.TYPE_1, NufftOpts(nmodes=nmodes, ntransf=ntransf, kernel_width=kernel_width))
+        try:
+            plan.set_spread_tuning(maxp, block)
+        except Exception:
+            plan.free()
+            continue
+        plan.setpts(list(coords))
+        plan.execute(data, out)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            plan.execute(data, out)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        timings.append((e0.elapsed_time(e1) / reps, list(block), int(maxp)))
+        plan.free()
+    timings.sort()
+    best = {"block": timings[0][1], "max_candidates": timings[0][2], "ms": round(timings[0][0], 4),
+            "timings": [[round(t, 4), b, m] for t, b, m in timings]}
+    if use_cache:
+        cache = _load()
+        cache[key] = best
+        _store(cache)
+    return dict(best, cached=False)
+
+
+def apply(plan: NufftPlan, choice: dict) -> None:
+    """Applies a tuner choice to a plan (before its setpts)."""
+    plan.set_spread_tuning(int(choice["max_candidates"]), tuple(choice["block"]))

@@ -25,6 +25,16 @@ int sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x, c
                  void* out, void* workspace, size_t workspace_bytes, cudaStream_t s);
 int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps,
                          const void* kernel, void* out, cudaStream_t s);
+int sense_normal_batched(int dim, const int64_t* shape, int64_t nframes, int64_t ncoils, const void* x,
+                         const void* smaps, const void* kernels, void* out, void* workspace, size_t workspace_bytes,
+                         cudaStream_t s);
+int transform_toeplitz_kernels(int dim, const int64_t* kshape, int64_t nframes, const void* kin, void* kout,
+                               cudaStream_t s);
+size_t cgb_state_bytes(int64_t nframes);
+int cgb_init(int64_t n, int64_t nf, const void* b, const void* Ax, void* r, void* p, void* state, double tol,
+             cudaStream_t s);
+int cgb_step(int64_t n, int64_t nf, void* x, void* r, void* p, const void* Ap, void* state, cudaStream_t s);
+int cgb_read_state(const void* state, int64_t nf, double* rzold, int64_t* iters, int* converged, cudaStream_t s);
 size_t cg_state_bytes();
 int cg_init(int64_t n, const void* b, const void* Ax, void* r, void* p, void* state, double tol, cudaStream_t s);
 int cg_step(int64_t n, void* x, void* r, void* p, const void* Ap, void* state, cudaStream_t s);
@@ -99,6 +109,26 @@ int hb_nufft_execute(hb_nufft_plan plan, const void* in, void* out, void* stream
     })
 }
 
+int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block_z, int block_y, int block_x) {
+    HB_GUARD({
+        if (!plan) {
+            hb::set_error("plan is null");
+            return HB_ERR_INVALID_ARG;
+        }
+        return hb::plan_set_spread_tuning(&plan->p, max_candidates, block_z, block_y, block_x);
+    })
+}
+
+int hb_nufft_coord_grad(hb_nufft_plan plan, const void* modes, const void* h, float* grad, void* stream) {
+    HB_GUARD({
+        if (!plan) {
+            hb::set_error("plan is null");
+            return HB_ERR_INVALID_ARG;
+        }
+        return hb::plan_coord_grad(&plan->p, (const float2*)modes, (const float2*)h, grad, as_stream(stream));
+    })
+}
+
 int hb_nufft_destroy(hb_nufft_plan plan) {
     HB_GUARD({
         if (!plan) return HB_OK;
@@ -165,6 +195,38 @@ int hb_sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x
 int hb_sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps,
                             const void* kernel, void* out, void* stream) {
     HB_GUARD({ return hb::sense_normal_noalloc(dim, shape, ncoils, x, smaps, kernel, out, as_stream(stream)); })
+}
+
+int hb_sense_normal_batched(int dim, const int64_t* shape, int64_t nframes, int64_t ncoils, const void* x,
+                            const void* smaps, const void* kernels, void* out, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+    HB_GUARD({
+        return hb::sense_normal_batched(dim, shape, nframes, ncoils, x, smaps, kernels, out, workspace, workspace_bytes,
+                                        as_stream(stream));
+    })
+}
+
+int hb_transform_toeplitz_kernels(int dim, const int64_t* kernel_shape, int64_t nframes, const void* kernels_in,
+                                  void* kernels_out, void* stream) {
+    HB_GUARD({
+        return hb::transform_toeplitz_kernels(dim, kernel_shape, nframes, kernels_in, kernels_out, as_stream(stream));
+    })
+}
+
+size_t hb_cgb_state_bytes(int64_t nframes) { return hb::cgb_state_bytes(nframes); }
+
+int hb_cgb_init(int64_t n, int64_t nframes, const void* b, const void* Ax, void* r, void* p, void* state, double tol,
+                void* stream) {
+    HB_GUARD({ return hb::cgb_init(n, nframes, b, Ax, r, p, state, tol, as_stream(stream)); })
+}
+
+int hb_cgb_step(int64_t n, int64_t nframes, void* x, void* r, void* p, const void* Ap, void* state, void* stream) {
+    HB_GUARD({ return hb::cgb_step(n, nframes, x, r, p, Ap, state, as_stream(stream)); })
+}
+
+int hb_cgb_read_state(const void* state, int64_t nframes, double* rzold, int64_t* iters, int* converged,
+                      void* stream) {
+    HB_GUARD({ return hb::cgb_read_state(state, nframes, rzold, iters, converged, as_stream(stream)); })
 }
 
 size_t hb_cg_state_bytes(void) { return hb::cg_state_bytes(); }

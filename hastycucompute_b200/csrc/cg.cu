@@ -79,8 +79,16 @@ __device__ __forceinline__ bool finish_reduction(double part, double* partial, u
     return true;
 }
 
+// Every kernel below serves gridDim.y independent systems (frames): system f uses vector segment
+// [f*n, (f+1)*n) and state st[f]; one system is gridDim.y == 1.
 __global__ void __launch_bounds__(kRedThreads) k_cg_init(int64_t n, const float2* __restrict__ b, const float2* __restrict__ Ax,
                                                           float2* __restrict__ r, float2* __restrict__ p, CgState* st, double tol) {
+    const int64_t fo = (int64_t)blockIdx.y * n;
+    b += fo;
+    Ax += fo;
+    r += fo;
+    p += fo;
+    st += blockIdx.y;
     double part = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float2 v = csub(b[i], Ax[i]);
@@ -102,6 +110,10 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_init(int64_t n, const float2
 
 __global__ void __launch_bounds__(kRedThreads) k_cg_alpha(int64_t n, const float2* __restrict__ p, const float2* __restrict__ Ap,
                                                            CgState* st) {
+    const int64_t fo = (int64_t)blockIdx.y * n;
+    p += fo;
+    Ap += fo;
+    st += blockIdx.y;
     double part = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float2 a = p[i], c = Ap[i];
@@ -119,6 +131,12 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_alpha(int64_t n, const float
 __global__ void __launch_bounds__(kRedThreads) k_cg_update(int64_t n, float2* __restrict__ x, float2* __restrict__ r,
                                                             const float2* __restrict__ p, const float2* __restrict__ Ap,
                                                             CgState* st) {
+    const int64_t fo = (int64_t)blockIdx.y * n;
+    x += fo;
+    r += fo;
+    p += fo;
+    Ap += fo;
+    st += blockIdx.y;
     if (!st->run) return;
     const float alpha = (float)st->alpha;
     double part = 0;
@@ -143,6 +161,10 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_update(int64_t n, float2* __
 
 __global__ void __launch_bounds__(kRedThreads) k_cg_dir(int64_t n, const float2* __restrict__ r, float2* __restrict__ p,
                                                          const CgState* st) {
+    const int64_t fo = (int64_t)blockIdx.y * n;
+    r += fo;
+    p += fo;
+    st += blockIdx.y;
     if (!st->run) return;
     const float beta = (float)st->beta;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -171,6 +193,43 @@ __global__ void __launch_bounds__(kRedThreads) k_vdot_real(int64_t n, const floa
 }
 
 size_t cg_state_bytes() { return sizeof(CgState); }
+size_t cgb_state_bytes(int64_t nframes) { return sizeof(CgState) * (size_t)std::max<int64_t>(nframes, 1); }
+
+int cgb_init(int64_t n, int64_t nf, const void* b, const void* Ax, void* r, void* p, void* state, double tol,
+             cudaStream_t s) {
+    HB_REQUIRE(n >= 1 && nf >= 1 && nf <= 65535, HB_ERR_INVALID_ARG, "n >= 1 and 1 <= nframes <= 65535");
+    HB_REQUIRE(b && Ax && r && p && state, HB_ERR_INVALID_ARG, "null argument");
+    HB_CUDA(cudaMemsetAsync(state, 0, sizeof(CgState) * (size_t)nf, s));
+    dim3 grid(red_blocks(n), (unsigned)nf);
+    k_cg_init<<<grid, kRedThreads, 0, s>>>(n, (const float2*)b, (const float2*)Ax, (float2*)r, (float2*)p,
+                                          (CgState*)state, tol);
+    return check_launch("k_cg_init (frames)");
+}
+
+int cgb_step(int64_t n, int64_t nf, void* x, void* r, void* p, const void* Ap, void* state, cudaStream_t s) {
+    HB_REQUIRE(n >= 1 && nf >= 1 && nf <= 65535, HB_ERR_INVALID_ARG, "n >= 1 and 1 <= nframes <= 65535");
+    HB_REQUIRE(x && r && p && Ap && state, HB_ERR_INVALID_ARG, "null argument");
+    dim3 grid(red_blocks(n), (unsigned)nf);
+    CgState* st = (CgState*)state;
+    TimedSection ts("cg_step", s);
+    k_cg_alpha<<<grid, kRedThreads, 0, s>>>(n, (const float2*)p, (const float2*)Ap, st);
+    k_cg_update<<<grid, kRedThreads, 0, s>>>(n, (float2*)x, (float2*)r, (const float2*)p, (const float2*)Ap, st);
+    k_cg_dir<<<grid, kRedThreads, 0, s>>>(n, (const float2*)r, (float2*)p, st);
+    return check_launch("cg_step (frames)");
+}
+
+int cgb_read_state(const void* state, int64_t nf, double* rzold, int64_t* iters, int* converged, cudaStream_t s) {
+    HB_REQUIRE(state && nf >= 1, HB_ERR_INVALID_ARG, "bad argument");
+    for (int64_t f = 0; f < nf; ++f) {
+        CgState h;
+        HB_CUDA(cudaMemcpyAsync(&h, (const CgState*)state + f, offsetof(CgState, partial), cudaMemcpyDeviceToHost, s));
+        HB_CUDA(cudaStreamSynchronize(s));
+        if (rzold) rzold[f] = h.rzold;
+        if (iters) iters[f] = h.iters;
+        if (converged) converged[f] = (h.run == 0) || (sqrt(h.rzold) < h.tol);
+    }
+    return HB_OK;
+}
 
 int cg_init(int64_t n, const void* b, const void* Ax, void* r, void* p, void* state, double tol, cudaStream_t s) {
     HB_REQUIRE(n >= 1, HB_ERR_INVALID_ARG, "n must be >= 1");

@@ -99,11 +99,13 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseRedu
     extern __shared__ float2 smem2[];
     float2* tw = smem2;       // L
     float2* Y = smem2 + L;    // [L][CWp] transpose buffer
-    float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][Lout] running sums
-    float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * c.Lout : 0);  // kFusedK: [kMaxKCols][L]
+    float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][groups][Lout] running sums
+    float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * op.ngroups() * c.Lout : 0);  // kFusedK: [kMaxKCols][L]
     float2* Ss = Ks + (Op::kFusedK ? kMaxKCols * L : 0);          // kSenseReduce: [W][Lout]
 
     for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = c.tw[i];
+    if constexpr (Op::kSenseReduce)
+        for (int i = threadIdx.x; i < c.A_blk * op.ngroups() * c.Lout; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
 
     int64_t ab, eb_begin, eb_end;
     if (Op::kChunkLoop) {
@@ -265,19 +267,28 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseRedu
             }
             __syncthreads();
             const int tot = c.A_blk * c.Lout;
+            const int ng = op.ngroups();
             for (int idx = tid; idx < tot; idx += blockDim.x) {
                 const int o = idx % c.Lout, al = idx / c.Lout;
                 const int64_t a = a0 + al;
-                float2 sum = (eb == 0) ? make_float2(0.f, 0.f) : acc[idx];
-                if (a < c.A) {
-                    for (int el = 0; el < c.E_blk; ++el) {
-                        const int64_t e = e0 + el;
-                        if (e >= c.E) break;
-                        const int col = al * c.E_blk + el;
-                        sum = cadd(sum, op.product_s(Y[o * CWp + col], Ss[col * c.Lout + o]));
+                if (a >= c.A) continue;
+                float2 run = make_float2(0.f, 0.f);
+                int64_t gcur = op.group(e0);
+                for (int el = 0; el < c.E_blk; ++el) {
+                    const int64_t e = e0 + el;
+                    if (e >= c.E) break;
+                    const int64_t gg = op.group(e);
+                    if (gg != gcur) {
+                        float2* dst = acc + ((int64_t)al * ng + gcur) * c.Lout + o;
+                        *dst = cadd(*dst, run);
+                        run = make_float2(0.f, 0.f);
+                        gcur = gg;
                     }
+                    const int col = al * c.E_blk + el;
+                    run = cadd(run, op.product_s(Y[o * CWp + col], Ss[col * c.Lout + o]));
                 }
-                acc[idx] = sum;
+                float2* dst = acc + ((int64_t)al * ng + gcur) * c.Lout + o;
+                *dst = cadd(*dst, run);
             }
         } else {
             if (colok2) {
@@ -293,11 +304,13 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseRedu
         __syncthreads();
     }
     if constexpr (Op::kSenseReduce) {
-        const int tot = c.A_blk * c.Lout;
+        __syncthreads();
+        const int ng = op.ngroups();
+        const int tot = c.A_blk * ng * c.Lout;
         for (int idx = tid; idx < tot; idx += blockDim.x) {
-            const int o = idx % c.Lout, al = idx / c.Lout;
+            const int o = idx % c.Lout, rest = idx / c.Lout, gg = rest % ng, al = rest / ng;
             const int64_t a = a0 + al;
-            if (a < c.A) op.write_row(a, o, acc[idx]);
+            if (a < c.A) op.write_row(a, o, gg, acc[idx]);
         }
     }
 }

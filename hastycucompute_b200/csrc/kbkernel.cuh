@@ -42,6 +42,13 @@ __device__ __forceinline__ float kb_tap(const float* coef, int deg, int d, float
     for (int m = deg - 1; m >= 0; --m) acc = fmaf(acc, s, c[m]);
     return acc;
 }
+// Device: d phi / dz for tap d (= 2 dP/ds, since z = d - w/2 + (s+1)/2).
+__device__ __forceinline__ float kb_tap_deriv(const float* coef, int deg, int d, float s) {
+    const float* c = coef + d * (kMaxDeg + 1);
+    float acc = (float)deg * c[deg];
+    for (int m = deg - 1; m >= 1; --m) acc = fmaf(acc, s, (float)m * c[m]);
+    return 2.f * acc;
+}
 #endif
 
 }  // namespace hb

@@ -651,24 +651,165 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
                     int gz = i0[0] + dz;
                     if (gz >= nf0) gz -= nf0;
                     const float wzv = wts[dz];
+                    unsigned rowbase[W];
 #pragma unroll
                     for (int dy = 0; dy < W; ++dy) {
-                        if (dy < wy) {
-                            int gy = i0[1] + dy;
-                            if (gy >= nf1) gy -= nf1;
-                            const float wzy = wzv * wts[kMaxWidth + dy];
-                            const unsigned rowbase = ((unsigned)gz * (unsigned)nf1 + (unsigned)gy) * rowstride;
+                        int gy = i0[1] + dy;
+                        if (gy >= nf1) gy -= nf1;
+                        rowbase[dy] = ((unsigned)gz * (unsigned)nf1 + (unsigned)gy) * rowstride;
+                    }
+                    if constexpr (W <= 6) {
+                        // issue the whole W x W slab of gathers before any multiply
+                        float2 v[W * W];
+#pragma unroll
+                        for (int dy = 0; dy < W; ++dy)
+#pragma unroll
+                            for (int dx = 0; dx < W; ++dx)
+                                v[dy * W + dx] = dy < wy ? gridc[rowbase[dy] + colofs[dx]] : make_float2(0.f, 0.f);
+#pragma unroll
+                        for (int dy = 0; dy < W; ++dy) {
+                            const float wzy = dy < wy ? wzv * wts[kMaxWidth + dy] : 0.f;
 #pragma unroll
                             for (int dx = 0; dx < W; ++dx) {
-                                const float2 v = gridc[rowbase + colofs[dx]];
                                 const float wgt = wzy * wx[dx];
-                                ar = fmaf(wgt, v.x, ar);
-                                ai = fmaf(wgt, v.y, ai);
+                                ar = fmaf(wgt, v[dy * W + dx].x, ar);
+                                ai = fmaf(wgt, v[dy * W + dx].y, ai);
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int dy = 0; dy < W; ++dy) {
+                            if (dy < wy) {
+                                const float wzy = wzv * wts[kMaxWidth + dy];
+                                float2 v[W];
+#pragma unroll
+                                for (int dx = 0; dx < W; ++dx) v[dx] = gridc[rowbase[dy] + colofs[dx]];
+#pragma unroll
+                                for (int dx = 0; dx < W; ++dx) {
+                                    const float wgt = wzy * wx[dx];
+                                    ar = fmaf(wgt, v[dx].x, ar);
+                                    ai = fmaf(wgt, v[dx].y, ai);
+                                }
                             }
                         }
                     }
                 }
                 a.out[(int64_t)(cc0 + coil) * g.M + pj] = make_float2(ar, ai);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ---- coordinate gradient by kernel-derivative interpolation ---------------------------------
+// grad_x[a][j] = -(nf_a / 2 pi) Re( sum_c h[c][j] sum_l G_c[l] dphi_a(l - u_j) prod_{b!=a} phi_b(l - u_j) )
+// G is the plan's fine grid after the type-2 passes, h a per-point complex factor:
+//   type 2 (c = A f):      h = conj(dL/dc),          G = grid of f
+//   type 1 (f = B c):      h = conj(c),              G = grid of dL/df through the opposite-sign
+//                          type-2 passes (the adjoint of deapodise + FFT)
+// This is the exact derivative of the implemented gridding operator with respect to the points.
+template <int CC, int W>
+__global__ void __launch_bounds__(kGridThreads) k_interp_grad(const GridArgs a, const float2* __restrict__ h,
+                                                             float* __restrict__ grad, int gdim) {
+    extern __shared__ float sm[];
+    constexpr int NS = 32 / CC;
+    float* coef = sm;
+    float* wts_all = coef + kCoefFloats;                                  // [slot][3][kMaxWidth]
+    float* dwt_all = wts_all + kGridWarps * NS * kSlotFloats;            // [slot][3][kMaxWidth]
+    const GridGeom& g = a.g;
+    for (int i = threadIdx.x; i < kCoefFloats; i += blockDim.x) coef[i] = (&a.kb.coef[0][0])[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = lane / CC, coil = lane % CC;
+    float* wts = wts_all + (warp * NS + slot) * kSlotFloats;
+    float* dwt = dwt_all + (warp * NS + slot) * kSlotFloats;
+    const int64_t gwarp = (int64_t)blockIdx.x * kGridWarps + warp;
+    const int64_t nwarps = (int64_t)gridDim.x * kGridWarps;
+    const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
+    const int wz = g.wa[0], wy = g.wa[1];
+    for (int64_t base = gwarp * NS; base < g.M; base += nwarps * NS) {
+        const int64_t s = base + slot;
+        const bool valid = s < g.M;
+        int i0[3];
+        point_setup(a, coef, s, valid, coil, CC, wts, i0);
+        // derivative taps (unit axes keep 0)
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const int w = g.wa[ax];
+            if (w == 1) {
+                if (coil == 0) dwt[ax * kMaxWidth] = 0.f;
+                continue;
+            }
+            const float u = valid ? a.su[ax][s] : 0.f;
+            const float v = __fsub_rn(u, a.kb.hw);
+            const float t = __fsub_rn(ceilf(v), v);
+            const float sarg = fmaf(2.f, t, -1.f);
+            for (int d = coil; d < w; d += CC) dwt[ax * kMaxWidth + d] = kb_tap_deriv(coef, a.kb.deg, d, sarg);
+        }
+        __syncwarp();
+        float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+        int pj = 0;
+        if (valid) {
+            unsigned colofs[W];
+            float wx[W], dx_[W];
+#pragma unroll
+            for (int d = 0; d < W; ++d) {
+                int v = i0[2] + d;
+                if (v >= nf2) v -= nf2;
+                colofs[d] = (unsigned)v * (unsigned)g.C;
+                wx[d] = wts[2 * kMaxWidth + d];
+                dx_[d] = dwt[2 * kMaxWidth + d];
+            }
+            pj = a.perm[s];
+            const unsigned rowstride = (unsigned)nf2 * (unsigned)g.C;
+            for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
+                if (cc0 + coil >= g.C) break;
+                const float2* gridc = a.grid + cc0 + coil;
+                float2 az = make_float2(0.f, 0.f), ay = az, axx = az;
+                for (int dz = 0; dz < wz; ++dz) {
+                    int gz = i0[0] + dz;
+                    if (gz >= nf0) gz -= nf0;
+                    const float wzv = wts[dz], dzv = dwt[dz];
+#pragma unroll
+                    for (int dy = 0; dy < W; ++dy) {
+                        if (dy < wy) {
+                            int gy = i0[1] + dy;
+                            if (gy >= nf1) gy -= nf1;
+                            const float wyv = wts[kMaxWidth + dy], dyv = dwt[kMaxWidth + dy];
+                            const float c_zy = wzv * wyv, c_dz = dzv * wyv, c_dy = wzv * dyv;
+                            const unsigned rowbase = ((unsigned)gz * (unsigned)nf1 + (unsigned)gy) * rowstride;
+#pragma unroll
+                            for (int dx = 0; dx < W; ++dx) {
+                                const float2 v = gridc[rowbase + colofs[dx]];
+                                const float t0 = c_dz * wx[dx], t1 = c_dy * wx[dx], t2 = c_zy * dx_[dx];
+                                az.x = fmaf(t0, v.x, az.x);
+                                az.y = fmaf(t0, v.y, az.y);
+                                ay.x = fmaf(t1, v.x, ay.x);
+                                ay.y = fmaf(t1, v.y, ay.y);
+                                axx.x = fmaf(t2, v.x, axx.x);
+                                axx.y = fmaf(t2, v.y, axx.y);
+                            }
+                        }
+                    }
+                }
+                const float2 hv = h[(int64_t)(cc0 + coil) * g.M + pj];
+                r0 += hv.x * az.x - hv.y * az.y;
+                r1 += hv.x * ay.x - hv.y * ay.y;
+                r2 += hv.x * axx.x - hv.y * axx.y;
+            }
+        }
+        // sum over the CC lanes of this slot
+#pragma unroll
+        for (int o = CC / 2; o >= 1; o >>= 1) {
+            r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+            r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+            r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+        }
+        if (valid && coil == 0) {
+            const float r[3] = {r0, r1, r2};
+            for (int i = 0; i < gdim; ++i) {
+                const int ax = 3 - gdim + i;
+                grad[(int64_t)i * g.M + pj] = -r[ax] * g.scale[ax];
             }
         }
         __syncwarp();
@@ -698,10 +839,12 @@ struct OpModesIn {
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
     __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
+    __device__ __forceinline__ int64_t group(int64_t) const { return 0; }
+    __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const { dst[a * d_a + (int64_t)o * d_l + e] = v; }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
-    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
+    __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         float2* d = dst;
@@ -730,13 +873,15 @@ struct OpModesOut {
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
     __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
+    __device__ __forceinline__ int64_t group(int64_t) const { return 0; }
+    __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
         const float sc = d0[a / N1] * d1[a % N1] * d2[o];
         f[e * nm + a * N2 + o] = cscale(v, sc);
     }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
-    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
+    __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) { store(a, o, e, v); });
@@ -812,6 +957,11 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
         g.nf[ax] = unit ? 1 : fine_size(g.Nm[ax], p->sigma, w, g.T[ax]);
         g.nb[ax] = g.nf[ax] / g.T[ax];
         g.scale[ax] = (float)((double)g.nf[ax] / (2.0 * M_PI));
+    }
+    if (dim == 2) {
+        p->wb[0] = 1;
+        p->wb[1] = 4;
+        p->wb[2] = 8;
     }
     p->beta = kb_beta(w, p->sigma);
     const double fit_err = kb_fit(&p->kb, w, p->beta);
@@ -939,7 +1089,7 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             TileNbr tn;
             for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
             k_tile_extra_count<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins,
-                                                                                kSpreadMaxCand, ecnt);
+                                                                                p->maxp, ecnt);
             if ((st = check_launch("k_tile_extra_count")) != HB_OK) break;
             if ((st = exclusive_scan_int(ecnt, eoff, p->nbins, s)) != HB_OK) break;
             int n_extra = 0, err = 0;
@@ -996,7 +1146,7 @@ static GridArgs grid_args(const NufftPlan* p) {
     a.inT = p->inT;
     a.grid = p->X;
     a.extra = p->extra;
-    a.maxp = kSpreadMaxCand;
+    a.maxp = p->maxp;
     a.kb = p->kb;
     return a;
 }
@@ -1007,7 +1157,7 @@ static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t 
     const int cells = g.T[0] * g.T[1] * g.T[2];
     if (cells == 512 && g.dim >= 2) {
         // output-stationary kernel: one thread per cell of an 8x8x8 (3-D) or 16x32 (2-D) tile
-        SpreadTileShape wb = g.dim == 3 ? SpreadTileShape{2, 4, 4} : SpreadTileShape{1, 4, 8};
+        SpreadTileShape wb{p->wb[0], p->wb[1], p->wb[2]};
         const size_t smem = sizeof(float) * (kCoefFloats + (size_t)kSpreadChunk * 3 * kMaxWidth) +
                             sizeof(float2) * (size_t)kSpreadChunk * CC + sizeof(int) * kSpreadChunk * 8;
         HB_CUDA(cudaFuncSetAttribute(k_spread_reg<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1082,6 +1232,37 @@ static int dispatch_cc(int cc, const NufftPlan* p, const GridArgs& a, cudaStream
     }
 }
 
+// Type-2 passes: caller modes [C][N..] -> fine grid (returned in *G, one of the plan buffers).
+static int type2_grid(NufftPlan* p, const float2* in, float2** G, cudaStream_t s) {
+    const GridGeom& g = p->g;
+    const int C = g.C;
+    const int64_t nm = g.Nm[0] * g.Nm[1] * g.Nm[2];
+    const bool inv = p->sign > 0;
+    const int64_t h0 = g.Nm[0] / 2, h1 = g.Nm[1] / 2, h2 = g.Nm[2] / 2;
+    const int npass = 1 + (g.nf[1] > 1) + (g.nf[0] > 1);
+    float2* cur = (npass % 2 == 1) ? p->X : p->Y;
+    float2* other = (cur == p->X) ? p->Y : p->X;
+    {
+        OpModesIn op{in, cur, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm, (int64_t)g.nf[2] * C, C};
+        HB_TRY(launch_fft_pass(op, p->fl[2], g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv, 0, s,
+                               "type2 axis2"));
+    }
+    if (g.nf[1] > 1) {
+        const int64_t E = (int64_t)g.nf[2] * C;
+        OpStrided op{cur, other, g.Nm[1] * E, E, (int64_t)g.nf[1] * E, E, 1.0f};
+        HB_TRY(launch_fft_pass(op, p->fl[1], g.Nm[0], E, (int)g.Nm[1], (int)-h1, g.nf[1], 0, inv, 0, s, "type2 axis1"));
+        std::swap(cur, other);
+    }
+    if (g.nf[0] > 1) {
+        const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
+        OpStrided op{cur, other, 0, E, 0, E, 1.0f};
+        HB_TRY(launch_fft_pass(op, p->fl[0], 1, E, (int)g.Nm[0], (int)-h0, g.nf[0], 0, inv, 0, s, "type2 axis0"));
+        std::swap(cur, other);
+    }
+    *G = cur;
+    return HB_OK;
+}
+
 int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
     HB_REQUIRE(p->pts_set, HB_ERR_STATE, "execute called before setpts");
     const GridGeom& g = p->g;
@@ -1129,34 +1310,76 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
         return HB_OK;
     }
 
-    // type 2: passes x, y, z then interpolate from X
-    const int npass = 1 + (g.nf[1] > 1) + (g.nf[0] > 1);
-    float2* cur = (npass % 2 == 1) ? p->X : p->Y;
-    float2* other = (cur == p->X) ? p->Y : p->X;
-    {
-        OpModesIn op{in, cur, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm, (int64_t)g.nf[2] * C, C};
-        HB_TRY(launch_fft_pass(op, p->fl[2], g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv, 0, s,
-                               "type2 axis2"));
-    }
-    if (g.nf[1] > 1) {
-        const int64_t E = (int64_t)g.nf[2] * C;
-        OpStrided op{cur, other, g.Nm[1] * E, E, (int64_t)g.nf[1] * E, E, 1.0f};
-        HB_TRY(launch_fft_pass(op, p->fl[1], g.Nm[0], E, (int)g.Nm[1], (int)-h1, g.nf[1], 0, inv, 0, s, "type2 axis1"));
-        std::swap(cur, other);
-    }
-    if (g.nf[0] > 1) {
-        const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
-        OpStrided op{cur, other, 0, E, 0, E, 1.0f};
-        HB_TRY(launch_fft_pass(op, p->fl[0], 1, E, (int)g.Nm[0], (int)-h0, g.nf[0], 0, inv, 0, s, "type2 axis0"));
-        std::swap(cur, other);
-    }
+    // type 2: passes x, y, z into the fine grid, then interpolate
+    float2* G = nullptr;
+    HB_TRY(type2_grid(p, in, &G, s));
     if (M > 0) {
         GridArgs a = grid_args(p);
-        a.grid = cur;
+        a.grid = G;
         a.out = out;
         HB_TRY(dispatch_cc(spread_cc(g), p, a, s, false));
     }
     return HB_OK;
+}
+
+template <int CC, int W>
+static int launch_grad_w(const NufftPlan* p, const GridArgs& a, const float2* h, float* grad, cudaStream_t s) {
+    const int64_t per_block = (int64_t)kGridWarps * (32 / CC);
+    int64_t blocks = ceil_div(std::max<int64_t>(p->g.M, 1), per_block);
+    blocks = std::min<int64_t>(blocks, (int64_t)kNumSMs * 64);
+    const size_t smem = sizeof(float) * (kCoefFloats + (size_t)2 * kGridWarps * (32 / CC) * kSlotFloats);
+    HB_CUDA(cudaFuncSetAttribute(k_interp_grad<CC, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TimedSection ts("interp_grad", s);
+    k_interp_grad<CC, W><<<(unsigned)blocks, kGridThreads, smem, s>>>(a, h, grad, p->g.dim);
+    return check_launch("k_interp_grad");
+}
+
+template <int CC>
+static int launch_grad_cc(const NufftPlan* p, const GridArgs& a, const float2* h, float* grad, cudaStream_t s) {
+    switch (p->kb.w) {
+        case 2: return launch_grad_w<CC, 2>(p, a, h, grad, s);
+        case 3: return launch_grad_w<CC, 3>(p, a, h, grad, s);
+        case 4: return launch_grad_w<CC, 4>(p, a, h, grad, s);
+        case 5: return launch_grad_w<CC, 5>(p, a, h, grad, s);
+        case 6: return launch_grad_w<CC, 6>(p, a, h, grad, s);
+        case 7: return launch_grad_w<CC, 7>(p, a, h, grad, s);
+        case 8: return launch_grad_w<CC, 8>(p, a, h, grad, s);
+        default: return HB_ERR_INVALID_ARG;
+    }
+}
+
+int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx) {
+    HB_REQUIRE(!p->pts_set, HB_ERR_STATE, "set the spread tuning before setpts");
+    HB_REQUIRE(maxp >= 32 && maxp <= (1 << 16), HB_ERR_INVALID_ARG, "max candidates must be in [32, 65536]");
+    const int b[3] = {bz, by, bx};
+    HB_REQUIRE(bz * by * bx == 32, HB_ERR_INVALID_ARG, "warp block must hold 32 cells");
+    for (int ax = 0; ax < 3; ++ax) {
+        HB_REQUIRE(b[ax] >= 1 && p->g.T[ax] % b[ax] == 0, HB_ERR_INVALID_ARG, "warp block must tile the spread tile");
+        HB_REQUIRE(p->g.T[ax] > 1 || b[ax] == 1, HB_ERR_INVALID_ARG, "unit axes take a block edge of 1");
+    }
+    p->maxp = maxp;
+    for (int ax = 0; ax < 3; ++ax) p->wb[ax] = b[ax];
+    return HB_OK;
+}
+
+int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s) {
+    HB_REQUIRE(p->type == 2, HB_ERR_INVALID_ARG, "coordinate gradient needs a type-2 plan");
+    HB_REQUIRE(p->pts_set, HB_ERR_STATE, "coordinate gradient called before setpts");
+    HB_REQUIRE(p->kb.w <= 8, HB_ERR_INVALID_ARG, "coordinate gradient supports kernel widths up to 8");
+    HB_REQUIRE(modes && grad && (h || p->g.M == 0), HB_ERR_INVALID_ARG, "null argument");
+    if (p->g.M == 0) return HB_OK;
+    float2* G = nullptr;
+    HB_TRY(type2_grid(p, modes, &G, s));
+    GridArgs a = grid_args(p);
+    a.grid = G;
+    switch (spread_cc(p->g)) {
+        case 1: return launch_grad_cc<1>(p, a, h, grad, s);
+        case 2: return launch_grad_cc<2>(p, a, h, grad, s);
+        case 4: return launch_grad_cc<4>(p, a, h, grad, s);
+        case 8: return launch_grad_cc<8>(p, a, h, grad, s);
+        case 16: return launch_grad_cc<16>(p, a, h, grad, s);
+        default: return launch_grad_cc<32>(p, a, h, grad, s);
+    }
 }
 
 void plan_free(NufftPlan* p) {

@@ -54,6 +54,9 @@ struct NufftPlan {
     int64_t extra_cap = 0;
     int* d_err = nullptr;
     bool pts_set = false;
+    // spreading knobs (autotuned): candidates per subproblem and the warp's cell block
+    int maxp = 1024;
+    int wb[3] = {2, 4, 4};
     size_t device_bytes = 0;
 };
 
@@ -64,6 +67,8 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
               int width, double upsampfac, int method);
 int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const float* c2, cudaStream_t s);
 int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s);
+int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s);
+int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx);
 void plan_free(NufftPlan* p);
 
 // Pieces reused by the Toeplitz kernel builder.

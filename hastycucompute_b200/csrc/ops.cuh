@@ -26,12 +26,14 @@ struct OpStrided {
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
     __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
+    __device__ __forceinline__ int64_t group(int64_t) const { return 0; }
+    __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
         dst[a * d_a + (int64_t)o * d_l + e] = cscale(v, scale);
     }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
-    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
+    __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         const float sc = scale;

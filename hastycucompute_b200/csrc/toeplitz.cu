@@ -101,10 +101,14 @@ struct OpToepIn {
     int in_m1, in_m2;
     float2* dst;
     int64_t N2, n, d_a, d_l;
+    // frames: column e = f * cpf + c reads in[c] and m1[f] (cpf = 0: in[e], shared m1)
+    int64_t cpf;
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
         const int64_t idx = a * N2 + l;
-        float2 v = in[e * n + idx];
-        if (m1) v = mult_typed(v, m1[idx], in_m1);
+        const int64_t ei = cpf ? e % cpf : e;
+        const int64_t m1o = cpf ? (e / cpf) * n : 0;
+        float2 v = in[ei * n + idx];
+        if (m1) v = mult_typed(v, m1[m1o + idx], in_m1);
         if (m2) v = mult_typed(v, m2[idx], in_m2);
         return v;
     }
@@ -112,10 +116,12 @@ struct OpToepIn {
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
     __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
+    __device__ __forceinline__ int64_t group(int64_t) const { return 0; }
+    __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const { dst[a * d_a + (int64_t)o * d_l + e] = v; }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
-    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
+    __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         float2* d = dst;
@@ -141,10 +147,12 @@ struct OpToepMid {
     __device__ __forceinline__ const float2* kptr(int64_t kc) const { return kt + kc * Lk; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
     __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
+    __device__ __forceinline__ int64_t group(int64_t) const { return 0; }
+    __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int pos, int64_t e) const { return kt[(e / B) * Lk + pos]; }
     __device__ __forceinline__ void store(int64_t, int o, int64_t e, float2 v) const { buf[(int64_t)o * E + e] = v; }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
-    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
+    __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         float2* d = buf;
@@ -173,6 +181,8 @@ struct OpToepOutFlat {
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
     __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
+    __device__ __forceinline__ int64_t group(int64_t) const { return 0; }
+    __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
         const int64_t idx = a * N2 + o;
@@ -184,7 +194,7 @@ struct OpToepOutFlat {
         *dst = v;
     }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
-    __device__ __forceinline__ void write_row(int64_t, int, float2) const {}
+    __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int, int,
                                                 float2*) const {
         for_each_output<true>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) { store(a, o, e, v); });
@@ -192,8 +202,9 @@ struct OpToepOutFlat {
     __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
 };
 
-// Last pass of the SENSE normal operator: out[a][o] = sum_b conj(S_b[a][o]) * v_b[a][o]. The CTA
-// walks every batch chunk of its rows and keeps the running sum in shared memory (extra).
+// Last pass of the SENSE normal operator: out[f][a][o] = sum_c conj(S_c[a][o]) * v_{f,c}[a][o],
+// columns e = f * cpf + c (one frame when cpf = B). The CTA walks every batch chunk of its rows and
+// keeps one running sum per (row, frame) in shared memory (extra).
 struct OpToepOutSense {
     static constexpr bool kLoadLFast = false;
     static constexpr bool kStoreLFast = false;
@@ -205,19 +216,29 @@ struct OpToepOutSense {
     const float2* smaps;
     float2* out;
     int64_t N2, n;
+    int64_t cpf;  // coils per frame
+    int nfr;      // frames
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
     __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
-    __device__ __forceinline__ const float2* srow(int64_t a, int64_t e) const { return smaps + e * n + a * N2; }
+    __device__ __forceinline__ const float2* srow(int64_t a, int64_t e) const { return smaps + (e % cpf) * n + a * N2; }
     __device__ __forceinline__ float2 product_s(float2 v, float2 sv) const { return cmulc(v, sv); }
+    __device__ __forceinline__ int64_t group(int64_t e) const { return e / cpf; }
+    __device__ __forceinline__ int ngroups() const { return nfr; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t, int, int64_t, float2) const {}
     __device__ __forceinline__ float2 product(int64_t a, int o, int64_t e, float2 v) const {
-        return cmulc(v, smaps[e * n + a * N2 + o]);
+        return cmulc(v, smaps[(e % cpf) * n + a * N2 + o]);
     }
-    __device__ __forceinline__ void write_row(int64_t a, int o, float2 v) const { out[a * N2 + o] = v; }
+    __device__ __forceinline__ void write_row(int64_t a, int o, int g, float2 v) const { out[g * n + a * N2 + o] = v; }
+    // generic-kernel path: acc is [A_blk][nfr][Lout], zeroed on the first chunk
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int Ab, int Eb,
                                                 float2* acc) const {
+        const int ng = nfr;
+        if (e0 == 0) {
+            for (int i = threadIdx.x; i < Ab * ng * c.Lout; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+            __syncthreads();
+        }
         const int tot = Ab * c.Lout;
         for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
             const int o = idx % c.Lout, al = idx / c.Lout;
@@ -226,24 +247,33 @@ struct OpToepOutSense {
             int pos = (o + c.out_shift) % c.L;
             if (pos < 0) pos += c.L;
             const int64_t idx_img = a * N2 + o;
-            float2 sum = (e0 == 0) ? make_float2(0.f, 0.f) : acc[idx];
+            float2 run = make_float2(0.f, 0.f);
+            int64_t gcur = group(e0);
             for (int el = 0; el < Eb; ++el) {
                 const int64_t e = e0 + el;
                 if (e >= c.E) break;
+                const int64_t gg = group(e);
+                if (gg != gcur) {
+                    float2* dst = acc + ((int64_t)al * ng + gcur) * c.Lout + o;
+                    *dst = cadd(*dst, run);
+                    run = make_float2(0.f, 0.f);
+                    gcur = gg;
+                }
                 const float2 v = res[pos * c.Wp + al * Eb + el];
-                const float2 sv = smaps[e * n + idx_img];
-                sum = cadd(sum, cmulc(v, sv));
+                run = cadd(run, cmulc(v, smaps[(e % cpf) * n + idx_img]));
             }
-            acc[idx] = sum;
+            float2* dst = acc + ((int64_t)al * ng + gcur) * c.Lout + o;
+            *dst = cadd(*dst, run);
         }
     }
     __device__ __forceinline__ void finish(const PassCfg& c, int64_t a0, float2* acc) const {
-        const int tot = c.A_blk * c.Lout;
+        const int ng = nfr;
+        const int tot = c.A_blk * ng * c.Lout;
         for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-            const int o = idx % c.Lout, al = idx / c.Lout;
+            const int o = idx % c.Lout, rest = idx / c.Lout, gg = rest % ng, al = rest / ng;
             const int64_t a = a0 + al;
             if (a >= c.A) continue;
-            out[a * N2 + o] = acc[idx];
+            out[gg * n + a * N2 + o] = acc[idx];
         }
     }
 };
@@ -274,6 +304,7 @@ struct ToepArgs {
     const float2* m2;
     int io_mult, in_m1, out_m1, in_m2, out_m2, accumulate;
     bool sense;
+    int64_t frames = 1;  // SENSE over frames: t.B = frames * coils, kernels per frame
 };
 
 static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream_t s) {
@@ -287,9 +318,10 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
     HB_TRY(get_len(L1, &f1));
     if (t.dim == 3) HB_TRY(get_len(L0, &f0));
 
+    const int64_t cpf = a.sense ? B / a.frames : 0;  // coils per frame (SENSE)
     // P1: axis 2, pad N2 -> L2, forward
     {
-        OpToepIn op{a.in, a.m1, a.m2, a.in_m1, a.in_m2, W1, N2, t.n, (int64_t)L2 * B, B};
+        OpToepIn op{a.in, a.m1, a.m2, a.in_m1, a.in_m2, W1, N2, t.n, (int64_t)L2 * B, B, a.frames > 1 ? cpf : 0};
         HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "toeplitz P1"));
     }
     const int64_t E2 = (int64_t)L2 * B;
@@ -302,7 +334,7 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
         // P3: axis 0 fused, in place on W2
         {
             const int64_t E = (int64_t)L1 * E2;
-            OpToepMid op{W2, a.kt, E, B, L0};
+            OpToepMid op{W2, a.kt, E, a.frames > 1 ? cpf : B, L0};
             HB_TRY(launch_fft_pass(op, f0, 1, E, (int)N0, 0, (int)N0, (int)(N0 - 1), 0, 0, s, "toeplitz P3"));
         }
         // P4: axis 1 inverse, crop -> W1
@@ -312,15 +344,15 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
         }
     } else {
         // fused pass along axis 1, in place on W1 ([1][N1][L2][B])
-        OpToepMid op{W1, a.kt, E2, B, L1};
+        OpToepMid op{W1, a.kt, E2, a.frames > 1 ? cpf : B, L1};
         HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0, 0, s, "toeplitz P3"));
     }
     // P5: axis 2 inverse, crop, output ops
     {
         if (a.sense) {
-            OpToepOutSense op{W1, (int64_t)L2 * B, B, a.in, a.out, N2, t.n};
-            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1, sizeof(float2) * (size_t)N2, s,
-                                   "toeplitz P5 sense"));
+            OpToepOutSense op{W1, (int64_t)L2 * B, B, a.in, a.out, N2, t.n, cpf, (int)a.frames};
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1,
+                                   sizeof(float2) * (size_t)N2 * a.frames, s, "toeplitz P5 sense"));
         } else {
             OpToepOutFlat op{W1, (int64_t)L2 * B, B, a.in, a.m1, a.m2, a.io_mult, a.out_m1, a.out_m2, a.accumulate,
                              a.out, N2, t.n};
@@ -419,6 +451,64 @@ int sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x, c
     a.in_m2 = HB_MULT_NONE;
     a.sense = true;
     return toep_run(t, a, g.ptr, s);
+}
+
+int sense_normal_batched(int dim, const int64_t* shape, int64_t nframes, int64_t ncoils, const void* x,
+                         const void* smaps, const void* kernels, void* out, void* workspace, size_t workspace_bytes,
+                         cudaStream_t s) {
+    HB_REQUIRE(nframes >= 1 && ncoils >= 1, HB_ERR_INVALID_ARG, "nframes and ncoils must be >= 1");
+    ToepGeom t;
+    HB_TRY(toep_geom(&t, dim, shape, nframes * ncoils));
+    HB_REQUIRE(x && smaps && kernels && out, HB_ERR_INVALID_ARG, "x, smaps, kernels and out must be non-null");
+    HB_REQUIRE(out != x, HB_ERR_INVALID_ARG, "out must not alias x");
+    WsGuard g;
+    HB_TRY(get_workspace(t, workspace, workspace_bytes, s, &g));
+    ToepArgs a{};
+    a.in = (const float2*)smaps;
+    a.out = (float2*)out;
+    a.kt = (const float2*)kernels;
+    a.m1 = (const float2*)x;
+    a.m2 = nullptr;
+    a.in_m1 = HB_MULT_MULT;
+    a.in_m2 = HB_MULT_NONE;
+    a.sense = true;
+    a.frames = nframes;
+    return toep_run(t, a, g.ptr, s);
+}
+
+// Kt[(c * F + f) * R + r] = K_f[r][c] * scale : per-frame transpose [F][R][Cc] -> [Cc][F][R]
+__global__ void k_transpose_scale_frames(const float2* __restrict__ in, float2* __restrict__ out, int64_t R, int64_t Cc,
+                                         int64_t F, float scale) {
+    __shared__ float2 tile[32][33];
+    const int64_t f = blockIdx.z;
+    const int64_t c0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
+    const float2* src = in + f * R * Cc;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t r = r0 + j, c = c0 + threadIdx.x;
+        if (r < R && c < Cc) tile[j][threadIdx.x] = src[r * Cc + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t c = c0 + j, r = r0 + threadIdx.x;
+        if (r < R && c < Cc) out[(c * F + f) * R + r] = cscale(tile[threadIdx.x][j], scale);
+    }
+}
+
+int transform_toeplitz_kernels(int dim, const int64_t* kshape, int64_t nframes, const void* kin, void* kout,
+                               cudaStream_t s) {
+    HB_REQUIRE(dim == 2 || dim == 3, HB_ERR_INVALID_ARG, "Toeplitz kernel must be 2-D or 3-D");
+    HB_REQUIRE(kshape && kin && kout && nframes >= 1 && nframes <= 65535, HB_ERR_INVALID_ARG, "bad argument");
+    HB_REQUIRE(kin != kout, HB_ERR_INVALID_ARG, "kernel_in and kernel_out must not alias");
+    int64_t R = kshape[0], Cc = 1, tot = 1;
+    for (int i = 0; i < dim; ++i) {
+        HB_REQUIRE(kshape[i] >= 2 && kshape[i] % 2 == 0, HB_ERR_SHAPE, "kernel dimensions must be even (2N)");
+        tot *= kshape[i];
+        if (i > 0) Cc *= kshape[i];
+    }
+    const float scale = (float)(1.0 / (double)tot);
+    dim3 grid((unsigned)ceil_div(Cc, 32), (unsigned)ceil_div(R, 32), (unsigned)nframes);
+    k_transpose_scale_frames<<<grid, dim3(32, 8), 0, s>>>((const float2*)kin, (float2*)kout, R, Cc, nframes, scale);
+    return check_launch("transform_toeplitz_kernels");
 }
 
 int transform_toeplitz_kernel(int dim, const int64_t* kshape, const void* kin, void* kout, cudaStream_t s) {
@@ -603,7 +693,7 @@ int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const vo
     float2* W2 = d.ws + (size_t)N0 * N1 * L2 * B;
     const int64_t E2 = (int64_t)L2 * B;
     {
-        OpToepIn op{S, (const float2*)x, nullptr, HB_MULT_MULT, HB_MULT_NONE, W1, N2, t.n, E2, B};
+        OpToepIn op{S, (const float2*)x, nullptr, HB_MULT_MULT, HB_MULT_NONE, W1, N2, t.n, E2, B, 0};
         HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "noalloc P1"));
     }
     if (t.dim == 3) {
@@ -625,7 +715,7 @@ int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const vo
         HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0, 0, s, "noalloc P3"));
     }
     {
-        OpToepOutSense op{W1, E2, B, S, (float2*)out, N2, t.n};
+        OpToepOutSense op{W1, E2, B, S, (float2*)out, N2, t.n, B, 1};
         HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1, sizeof(float2) * (size_t)N2, s,
                                "noalloc P5 sense"));
     }

@@ -151,6 +151,16 @@ class NufftPlan:
             pass
 
     # -- extras ----------------------------------------------------------------------------------
+    def set_spread_tuning(self, max_candidates: int = 1024, block=(2, 4, 4)) -> None:
+        """Spreading knobs (before setpts): points per subproblem and the warp's cell block
+        (image order; 2-D plans take (1, by, bx))."""
+        if self.M is not None:
+            raise RuntimeError("set the spread tuning before setpts")
+        b = tuple(int(v) for v in block)
+        if len(b) == 2:
+            b = (1,) + b
+        _lib.call("hb_nufft_set_spread_tuning", self._h, int(max_candidates), *b)
+
     def info(self) -> PlanInfo:
         fine = (C.c_int64 * 3)()
         w = C.c_int()
@@ -182,3 +192,25 @@ def nufft_type2(coords: Sequence[torch.Tensor], image: torch.Tensor, **kw) -> to
     plan = NufftPlan(NufftType.TYPE_2, opts)
     plan.setpts(coords)
     return plan(image)
+
+
+def nufft_backward_cpu_over_cuda(dimshape: Sequence[int], input: torch.Tensor, coords: Sequence[torch.Tensor],
+                                 kernel_width: int = 0, tol: float = 1e-6) -> torch.Tensor:
+    """nufft_backward_cpu_over_cuda (cpp/corelib/lib/fft/nufft.cppm:316-382): adjoint NUFFT of host
+    data [T, M] at device coordinates, returned on the host as [T, *dimshape]. The reference moves
+    and transforms one row at a time with a device synchronisation around each; here all T rows go
+    in one pinned copy and one batched execute. tol 1e-6 is the reference's float default."""
+    if input.is_cuda:
+        raise ValueError("input must be a host tensor")
+    dev = coords[0].device
+    T = input.shape[0]
+    host = input.to(torch.complex64).contiguous().pin_memory()
+    d = host.to(dev, non_blocking=True)
+    plan = NufftPlan(NufftType.TYPE_1, NufftOpts(nmodes=tuple(dimshape), ntransf=T, tol=tol, kernel_width=kernel_width))
+    plan.setpts(list(coords))
+    out = plan(d)
+    res = torch.empty(out.shape, dtype=torch.complex64).pin_memory()
+    res.copy_(out, non_blocking=True)
+    torch.cuda.current_stream(dev).synchronize()
+    plan.free()
+    return res.to(input.dtype) if input.dtype != torch.complex64 and input.is_complex() else res

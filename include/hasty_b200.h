@@ -97,6 +97,23 @@ int hb_nufft_setpts(hb_nufft_plan plan, int64_t M, const float* coord0, const fl
  * Allocation free, graph capturable. */
 int hb_nufft_execute(hb_nufft_plan plan, const void* in, void* out, void* stream);
 
+/* Spreading knobs (no counterpart in the reference; set by the autotuner, before setpts): points
+ * per spread subproblem (32..65536, default 1024) and the cell block a warp owns inside a spread
+ * tile (32 cells; default 2x4x4 in 3-D, 1x4x8 in 2-D; each edge divides the tile edge, unit axes 1). */
+int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block_z, int block_y,
+                               int block_x);
+
+/* Coordinate gradient (no counterpart in the reference, which has no derivatives): with a
+ * type-2 plan (sign s) whose points are set, writes to grad ([dim][M] float, image order)
+ *   grad[i][j] = -(nf_i / 2 pi) Re( sum_c h[c][j] sum_l G_c[l] dPhi_i(l - u_j) )
+ * where G is the plan's fine grid of `modes` ([ntransf, N..]) after the type-2 passes and dPhi_i
+ * the kernel with its derivative along dimension i: the exact derivative of the implemented
+ * gridding operator with respect to the points. For c = A f (this plan) and a real loss L,
+ * h = conj(dL/dc) gives dL/dx. For f = B c (a type-1 plan of sign -s on the same points),
+ * modes = dL/df and h = conj(c) give dL/dx. Kernel widths up to 8. */
+int hb_nufft_coord_grad(hb_nufft_plan plan, const void* modes, const void* h, float* grad,
+                        void* stream);
+
 /* nufft_plan::free / ~nufft_plan, nufft.cppm:279-301. Safe on NULL. */
 int hb_nufft_destroy(hb_nufft_plan plan);
 
@@ -151,6 +168,20 @@ int hb_sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x
                     const void* smaps, const void* kernel, void* out,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---- frames: many systems in one launch per pass (no counterpart in the reference) -------
+ * hb_sense_normal over F frames that share the coil maps, each with its own Toeplitz kernel:
+ *   out[f] = sum_c conj(S_c) T_f(S_c x[f])     x, out: [F, N..]; smaps: [C, N..]
+ * kernels from hb_transform_toeplitz_kernels. All F*C columns run through each of the five passes
+ * in one launch. Workspace: hb_toeplitz_workspace_size(dim, shape, F*C). The per-frame loop it
+ * replaces is NORMAL_T_T1_OP::operator() (cpp/corelib/lib/mri/normal.cppm:65-88) once per frame. */
+int hb_sense_normal_batched(int dim, const int64_t* shape, int64_t nframes, int64_t ncoils,
+                            const void* x, const void* smaps, const void* kernels, void* out,
+                            void* workspace, size_t workspace_bytes, void* stream);
+/* transform_toeplitz_kernel (cpp/corelib/lib/fft/toeplitz.cppm:510-609) for F straight kernels
+ * [F, 2N..] at once, into the layout hb_sense_normal_batched reads. */
+int hb_transform_toeplitz_kernels(int dim, const int64_t* kernel_shape, int64_t nframes,
+                                  const void* kernels_in, void* kernels_out, void* stream);
+
 /* Allocation-free variant of hb_sense_normal (no counterpart in the reference). For callers
  * that cannot allocate device memory -- a runtime embedded in another framework that owns all
  * allocations, a driver layer handing out fixed buffers, code running where cudaMalloc is off
@@ -181,6 +212,16 @@ int hb_cg_step(int64_t n, void* x, void* r, void* p, const void* Ap, void* state
 /* Copies {rzold, iterations done, converged flag} to host (synchronises the stream). */
 int hb_cg_read_state(const void* state, double* rzold, int64_t* iters, int* converged,
                      void* stream);
+
+/* The same steps for F independent systems at once (vectors [F, n], one state block per frame,
+ * hb_cgb_state_bytes(F) bytes); each frame keeps its own scalars and its own early exit. */
+size_t hb_cgb_state_bytes(int64_t nframes);
+int hb_cgb_init(int64_t n, int64_t nframes, const void* b, const void* Ax, void* r, void* p,
+                void* state, double tol, void* stream);
+int hb_cgb_step(int64_t n, int64_t nframes, void* x, void* r, void* p, const void* Ap,
+                void* state, void* stream);
+int hb_cgb_read_state(const void* state, int64_t nframes, double* rzold, int64_t* iters,
+                      int* converged, void* stream);
 
 /* ---- vector helpers ------------------------------------------------------------------ */
 /* Re<a,b> in FP64, written to *result_dev (a device double). Deterministic order. */
