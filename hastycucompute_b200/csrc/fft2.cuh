@@ -71,6 +71,30 @@ __device__ __forceinline__ void dft_reg(float2* v, const float2* tw, int tws) {
     }
 }
 
+// DFT of size R whose inputs v[R/2..R) are zero: X[2m] = DFT_{R/2}(v)[m],
+// X[2m+1] = DFT_{R/2}(v_j W_R^j)[m].
+template <int R, bool INV>
+__device__ __forceinline__ void dft_reg_halfzero(float2* v, const float2* tw, int tws) {
+    if constexpr (R % 2 != 0 || R < 4) {
+        dft_reg<R, INV>(v, tw, tws);
+    } else {
+        constexpr int H = R / 2;
+        float2 a[H], b[H];
+#pragma unroll
+        for (int j = 0; j < H; ++j) {
+            a[j] = v[j];
+            b[j] = j == 0 ? v[0] : cmul(v[j], tw_get<INV>(tw, j * tws));
+        }
+        dft_reg<H, INV>(a, tw, tws * 2);
+        dft_reg<H, INV>(b, tw, tws * 2);
+#pragma unroll
+        for (int m = 0; m < H; ++m) {
+            v[2 * m] = a[m];
+            v[2 * m + 1] = b[m];
+        }
+    }
+}
+
 constexpr int kCW = 16;  // columns per CTA
 constexpr int kMaxKCols = 4;  // distinct kernel columns a fused CTA stages in shared memory
 
@@ -78,6 +102,11 @@ constexpr int kMaxKCols = 4;  // distinct kernel columns a fused CTA stages in s
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+// 16-byte variant (both addresses 16-byte aligned); bypasses L1.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
@@ -93,7 +122,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //   const float2* srow(int64_t a, int64_t e) const                      (kSenseReduce: the
 //       factor row of (a, e), staged per chunk; product_s(v, s) combines a value with it)
 template <int P, int Q, class Op>
-__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseReduce || Op::kFusedK) ? 2 : 3)) pass2_kernel(const Op op, const PassCfg c) {
+__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduce ? 2 : 3)) pass2_kernel(const Op op, const PassCfg c) {
     constexpr int L = P * Q;
     constexpr int CWp = kCW + 1;
     extern __shared__ float2 smem2[];
@@ -168,12 +197,20 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseRedu
                 if (l < 0) l += L;
                 v[j] = (colok && l < c.Lin) ? op.load(a, l, e) : make_float2(0.f, 0.f);
             }
+            // zero padding to 2x (Lin == L/2 at shift 0): only v[0..P/2) can be non-zero
+            const bool halfzero = (2 * c.Lin == L) && in_shift == 0;
             if (c.inverse) {
-                dft_reg<P, true>(v, tw, Q);
+                if (halfzero)
+                    dft_reg_halfzero<P, true>(v, tw, Q);
+                else
+                    dft_reg<P, true>(v, tw, Q);
 #pragma unroll
                 for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<true>(tw, t * k1));
             } else {
-                dft_reg<P, false>(v, tw, Q);
+                if (halfzero)
+                    dft_reg_halfzero<P, false>(v, tw, Q);
+                else
+                    dft_reg<P, false>(v, tw, Q);
 #pragma unroll
                 for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<false>(tw, t * k1));
             }
@@ -208,7 +245,6 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseRedu
             // multiply by the kernel at position k1 + P k2, inverse Q-point DFT over k2
             __syncthreads();  // everyone has read Y
             if (s2active) {
-#pragma unroll
                 if (k_staged) {
                     const float2* kc = Ks + (int)(op.kcol(e2) - kc0) * L;
 #pragma unroll
@@ -268,6 +304,20 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : ((Op::kSenseRedu
             __syncthreads();
             const int tot = c.A_blk * c.Lout;
             const int ng = op.ngroups();
+            if (ng == 1) {
+                // one frame: every column of the chunk adds into the row's single sum
+                for (int idx = tid; idx < tot; idx += blockDim.x) {
+                    const int o = idx % c.Lout, al = idx / c.Lout;
+                    if (a0 + al >= c.A) continue;
+                    const int ecount = (int)min((int64_t)c.E_blk, c.E - e0);
+                    float2 run = acc[idx];
+                    for (int el = 0; el < ecount; ++el) {
+                        const int col = al * c.E_blk + el;
+                        run = cadd(run, op.product_s(Y[o * CWp + col], Ss[col * c.Lout + o]));
+                    }
+                    acc[idx] = run;
+                }
+            } else
             for (int idx = tid; idx < tot; idx += blockDim.x) {
                 const int o = idx % c.Lout, al = idx / c.Lout;
                 const int64_t a = a0 + al;

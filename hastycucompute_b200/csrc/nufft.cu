@@ -409,30 +409,50 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
 
 // ---- output-stationary spreading ------------------------------------------------------------
 // One CTA owns one tile (one thread per cell) and keeps CC transforms of its cell in registers.
-// Candidate points are staged in shared memory in chunks (first cell relative to the tile, tap
-// weights, CC values); every thread then walks the chunk and accumulates the points whose
-// footprint covers its cell. A warp owns a compact block of cells (2x4x4 in 3-D, 4x8 in 2-D)
-// and skips a point with one vote when the footprint misses the whole block. No atomics except
-// for the extra chunks of dense tiles, which add their partial tile to the grid.
+// Candidate points pass through shared memory in chunks of kSpreadChunk, double-buffered: while
+// the CTA accumulates chunk i, its threads stage chunk i+1 -- one thread per (point, axis)
+// evaluates the w tap weights, the point's first cell relative to the tile and the warp blocks
+// its footprint meets along that axis, and the CC values arrive by cp.async. One barrier per
+// chunk. A warp owns a compact block of 32 cells (2x4x4 in 3-D, 4x8 in 2-D by default) and
+// skips a point with one vote when the footprint misses the block. The finished tile leaves
+// through shared memory, so each warp store covers whole runs of coils of the interleaved grid.
+// No atomics except for the extra chunks of dense tiles, which add their partial tile.
 constexpr int kSpreadChunk = 128;
+constexpr int kSpreadThreads = 512;
 
 struct SpreadTileShape {
     int bz, by, bx;  // warp block
 };
 
+// Shared-memory plan (in floats) after the kernel-polynomial copy: two staging buffers
+// {values float2[chunk][CC], taps float[chunk][3][kMaxWidth], first cells int[chunk] (3 bytes,
+// +16 biased), block masks uint2[chunk] (3 x 16 bits)}, reused at the end as per-warp output
+// tiles float2[32 cells][H + 1].
 template <int CC>
-__global__ void __launch_bounds__(512) k_spread_reg(const GridArgs a, int extra_mode, SpreadTileShape wb) {
-    extern __shared__ float sm[];
+struct SpreadSmem {
+    static constexpr int kVal = kSpreadChunk * CC * 2;
+    static constexpr int kW = kSpreadChunk * 3 * kMaxWidth;
+    static constexpr int kBuf = kVal + kW + 3 * kSpreadChunk;
+    static constexpr int kHalf = CC < 16 ? CC : 16;  // coils per output round
+    static constexpr int kOut = (kSpreadThreads / 32) * 32 * (kHalf + 1) * 2;
+    static constexpr int kFloats = kCoefFloats + (2 * kBuf > kOut ? 2 * kBuf : kOut);
+};
+
+// Bits lo/bs .. hi/bs (inclusive) of a block mask.
+__device__ __forceinline__ unsigned block_bits(int lo, int hi, int bs) {
+    return (2u << (hi / bs)) - (1u << (lo / bs));
+}
+
+template <int CC>
+__global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
+    k_spread_reg(const GridArgs a, int extra_mode, SpreadTileShape wb) {
+    using SM = SpreadSmem<CC>;
+    extern __shared__ float4 sm_f4[];
+    float* coef = reinterpret_cast<float*>(sm_f4);
+    float* region = coef + kCoefFloats;
+    __shared__ int s_start[8], s_pref[9], s_nbin;
     const GridGeom& g = a.g;
     const int T0 = g.T[0], T1 = g.T[1], T2 = g.T[2];
-    float* coef = sm;                                   // kCoefFloats
-    float* s_w = coef + kCoefFloats;                    // [chunk][3][kMaxWidth]
-    float2* s_val = (float2*)(s_w + kSpreadChunk * 3 * kMaxWidth);  // [chunk][CC]
-    int* s_rel = (int*)(s_val + kSpreadChunk * CC);     // [chunk][3]
-    float* s_sarg = (float*)(s_rel + kSpreadChunk * 3); // [chunk][3]
-    int* s_idx = (int*)(s_sarg + kSpreadChunk * 3);     // [chunk]
-    unsigned* s_mask = (unsigned*)(s_idx + kSpreadChunk); // [chunk] warps whose block the footprint meets
-    __shared__ int s_start[8], s_pref[9], s_nbin;
 
     int tile, chunk;
     if (extra_mode) {
@@ -444,17 +464,20 @@ __global__ void __launch_bounds__(512) k_spread_reg(const GridArgs a, int extra_
         chunk = 0;
     }
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
-    const int o0 = tz * T0, o1 = ty * T1, o2 = tx * T2;
+    const int org0 = tz * T0, org1 = ty * T1, org2 = tx * T2;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // this thread's cell
+    // this thread's cell and its warp's block
     const int nbx = T2 / wb.bx, nby = T1 / wb.by;
     const int bxi = warp % nbx, byi = (warp / nbx) % nby, bzi = warp / (nbx * nby);
     const int cz = bzi * wb.bz + lane / (wb.by * wb.bx);
     const int cy = byi * wb.by + (lane / wb.bx) % wb.by;
     const int cx = bxi * wb.bx + lane % wb.bx;
+    const int czb = cz + 16, cyb = cy + 16, cxb = cx + 16;
+    const unsigned mz = 1u << bzi, my = 1u << (16 + byi), mx = 1u << bxi;
     const int w0 = g.wa[0], w1 = g.wa[1], w2 = g.wa[2];
+    const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
 
-    for (int i = tid; i < kCoefFloats; i += blockDim.x) coef[i] = (&a.kb.coef[0][0])[i];
+    for (int i = tid; i < kCoefFloats; i += kSpreadThreads) coef[i] = (&a.kb.coef[0][0])[i];
     if (tid == 0) {
         int n = 0, acc = 0;
         for_each_nbr_bin(g.nb, tz, ty, tx, [&](int bin) {
@@ -468,138 +491,180 @@ __global__ void __launch_bounds__(512) k_spread_reg(const GridArgs a, int extra_
         s_nbin = n;
     }
     __syncthreads();
-    const int total = s_pref[s_nbin];
+    const int nbin = s_nbin;
+    const int total = s_pref[nbin];
     const int k_begin = chunk * a.maxp;
     const int k_end = min(total, k_begin + a.maxp);
     const float hw = a.kb.hw;
+    const bool vec = (g.C % 2) == 0;
+
+    // candidate k of this tile -> sorted point index
+    auto sorted_index = [&](int k) -> int {
+        int b = 0;
+#pragma unroll
+        for (int j = 1; j < 8; ++j) b += (j < nbin && s_pref[j] <= k) ? 1 : 0;
+        return s_start[b] + (k - s_pref[b]);
+    };
+
+    auto stage = [&](int base, int cc0, float* buf) {
+        const int n = min(kSpreadChunk, k_end - base);
+        float2* bval = reinterpret_cast<float2*>(buf);
+        float* bwt = buf + SM::kVal;
+        unsigned char* brel = reinterpret_cast<unsigned char*>(bwt + SM::kW);
+        unsigned short* bam = reinterpret_cast<unsigned short*>(brel + 4 * kSpreadChunk);
+        // the CC values of each point (asynchronous)
+        if constexpr (CC == 1) {
+            for (int q = tid; q < n; q += kSpreadThreads) {
+                if (cc0 < g.C) cp_async8(bval + q, a.inT + (int64_t)sorted_index(base + q) * g.C + cc0);
+            }
+        } else {
+            constexpr int CP = CC / 2;
+            for (int i = tid; i < n * CP; i += kSpreadThreads) {
+                const int q = i / CP, c = 2 * (i % CP);
+                float2* dst = bval + q * CC + c;
+                const int cg = cc0 + c;
+                const float2* src = a.inT + (int64_t)sorted_index(base + q) * g.C + cg;
+                if (vec && cg < g.C) {
+                    cp_async16(dst, src);
+                } else {
+                    if (cg < g.C) cp_async8(dst, src); else dst[0] = make_float2(0.f, 0.f);
+                    if (cg + 1 < g.C) cp_async8(dst + 1, src + 1); else dst[1] = make_float2(0.f, 0.f);
+                }
+            }
+        }
+        // per (point, axis): tap weights, first cell relative to the tile, warp blocks met
+        for (int i = tid; i < 3 * n; i += kSpreadThreads) {
+            const int q = i / 3, ax = i - 3 * q;
+            const int w = g.wa[ax];
+            float* wt = bwt + (q * 3 + ax) * kMaxWidth;
+            int relb = 16;
+            unsigned am = 1u;
+            if (w > 1) {
+                const float u = a.su[ax][sorted_index(base + q)];
+                const float v = __fsub_rn(u, hw);
+                const int ic = (int)ceilf(v);
+                const float sarg = fmaf(2.f, __fsub_rn((float)ic, v), -1.f);
+                const int nf = g.nf[ax], T = g.T[ax];
+                const int bs = ax == 0 ? wb.bz : (ax == 1 ? wb.by : wb.bx);
+                int iw = ic;
+                if (iw < 0) iw += nf;
+                if (iw >= nf) iw -= nf;
+                int rel = iw - (ax == 0 ? org0 : (ax == 1 ? org1 : org2));
+                if (rel < 0) rel += nf;
+                for (int d = 0; d < w; ++d) wt[d] = kb_tap(coef, a.kb.deg, d, sarg);
+                // footprint cells rel .. rel+w-1 (mod nf) inside [0, T)
+                am = 0u;
+                if (rel < T) {
+                    am |= block_bits(rel, min(rel + w - 1, T - 1), bs);
+                    relb = rel + 16;
+                } else {
+                    relb = max(rel - nf + 16, 0);  // a footprint reaching the tile starts >= -(w-1)
+                }
+                if (rel + w - 1 >= nf) am |= block_bits(0, min(rel + w - 1 - nf, T - 1), bs);
+            } else {
+                wt[0] = 1.f;
+            }
+            brel[q * 4 + ax] = (unsigned char)relb;
+            bam[q * 4 + ax] = (unsigned short)am;
+        }
+    };
 
     for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
         float ar[CC], ai[CC];
 #pragma unroll
         for (int c = 0; c < CC; ++c) ar[c] = ai[c] = 0.f;
-        for (int base = k_begin; base < k_end; base += kSpreadChunk) {
-            const int n = min(kSpreadChunk, k_end - base);
-            // stage A: sorted index, first cell relative to the tile, Horner argument
-            if (tid < n) {
-                const int k = base + tid;
-                int b = 0;
-                while (b + 1 < s_nbin && s_pref[b + 1] <= k) ++b;
-                const int s = s_start[b] + (k - s_pref[b]);
-                s_idx[tid] = s;
-                const int org[3] = {o0, o1, o2};
-#pragma unroll
-                for (int ax = 0; ax < 3; ++ax) {
-                    if (g.wa[ax] == 1) {
-                        s_rel[tid * 3 + ax] = 0;
-                        s_sarg[tid * 3 + ax] = 0.f;
-                        continue;
+        const int nch = (k_end - k_begin + kSpreadChunk - 1) / kSpreadChunk;
+        if (nch > 0) stage(k_begin, cc0, region);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        for (int it = 0; it < nch; ++it) {
+            const int base = k_begin + it * kSpreadChunk;
+            if (it + 1 < nch) stage(base + kSpreadChunk, cc0, region + ((it + 1) & 1) * SM::kBuf);
+            cp_async_commit();
+            // accumulate chunk it: each warp visits the points whose footprint meets its block
+            {
+                const int n = min(kSpreadChunk, k_end - base);
+                const float* buf = region + (it & 1) * SM::kBuf;
+                const float2* bval = reinterpret_cast<const float2*>(buf);
+                const float* bwt = buf + SM::kVal;
+                const int* brel = reinterpret_cast<const int*>(bwt + SM::kW);
+                const uint2* bam = reinterpret_cast<const uint2*>(brel + kSpreadChunk);
+                for (int q0 = 0; q0 < n; q0 += 32) {
+                    const int qq = q0 + lane;
+                    bool hit = false;
+                    if (qq < n) {
+                        const uint2 m = bam[qq];
+                        hit = (m.x & mz) && (m.x & my) && (m.y & mx);
                     }
-                    const float u = a.su[ax][s];
-                    const float v = __fsub_rn(u, hw);
-                    const int ic = (int)ceilf(v);
-                    const float t = __fsub_rn((float)ic, v);
-                    const int nf = g.nf[ax];
-                    int iw = ic;
-                    if (iw < 0) iw += nf;
-                    if (iw >= nf) iw -= nf;
-                    int rel = iw - org[ax];
-                    if (rel < 0) rel += nf;
-                    s_rel[tid * 3 + ax] = rel;
-                    s_sarg[tid * 3 + ax] = fmaf(2.f, t, -1.f);
-                }
-                // which warp blocks the footprint meets, per axis, then combined
-                const int bsz[3] = {wb.bz, wb.by, wb.bx};
-                const int nblk[3] = {T0 / wb.bz, T1 / wb.by, T2 / wb.bx};
-                unsigned am[3];
-#pragma unroll
-                for (int ax = 0; ax < 3; ++ax) {
-                    am[ax] = 0u;
-                    const int rel = s_rel[tid * 3 + ax], w = g.wa[ax], nf = g.nf[ax];
-                    for (int bi = 0; bi < nblk[ax]; ++bi)
-                        for (int cc = bi * bsz[ax]; cc < (bi + 1) * bsz[ax]; ++cc) {
-                            int d = cc - rel;
-                            if (d < 0) d += nf;
-                            if (d < w) {
-                                am[ax] |= 1u << bi;
-                                break;
-                            }
+                    unsigned bits = __ballot_sync(0xffffffffu, hit);
+                    while (bits) {
+                        const int q = q0 + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        const int pk = brel[q];
+                        int dz = czb - (pk & 0xff);
+                        int dy = cyb - ((pk >> 8) & 0xff);
+                        int dx = cxb - ((pk >> 16) & 0xff);
+                        if (dz < 0) dz += nf0;
+                        if (dy < 0) dy += nf1;
+                        if (dx < 0) dx += nf2;
+                        float wgt = 0.f;
+                        if (dz < w0 && dy < w1 && dx < w2) {
+                            const float* wq = bwt + q * 3 * kMaxWidth;
+                            wgt = wq[dz] * wq[kMaxWidth + dy] * wq[2 * kMaxWidth + dx];
                         }
-                }
-                unsigned m = 0u;
-                const int nw = nblk[0] * nblk[1] * nblk[2];
-                for (int wi = 0; wi < nw; ++wi) {
-                    const int xi = wi % nblk[2], yi = (wi / nblk[2]) % nblk[1], zi = wi / (nblk[2] * nblk[1]);
-                    if (((am[0] >> zi) & (am[1] >> yi) & (am[2] >> xi) & 1u) != 0u) m |= 1u << wi;
-                }
-                s_mask[tid] = m;
-            }
-            __syncthreads();
-            // stage B: tap weights and the CC values of every staged point
-            for (int i = tid; i < n * 3 * kMaxWidth; i += blockDim.x) {
-                const int q = i / (3 * kMaxWidth), r = i % (3 * kMaxWidth), ax = r / kMaxWidth, d = r % kMaxWidth;
-                const int w = g.wa[ax];
-                float val = 0.f;
-                if (d < w) val = (w == 1) ? 1.f : kb_tap(coef, a.kb.deg, d, s_sarg[q * 3 + ax]);
-                s_w[i] = val;
-            }
-            for (int i = tid; i < n * CC; i += blockDim.x) {
-                const int q = i / CC, c = i % CC;
-                s_val[i] = (cc0 + c < g.C) ? a.inT[(int64_t)s_idx[q] * g.C + cc0 + c] : make_float2(0.f, 0.f);
-            }
-            __syncthreads();
-            // accumulate: each warp visits only the staged points whose footprint meets its block
-            for (int q0 = 0; q0 < n; q0 += 32) {
-                const int qq = q0 + lane;
-                const bool hit = qq < n && ((s_mask[qq] >> warp) & 1u);
-                unsigned bits = __ballot_sync(0xffffffffu, hit);
-                while (bits) {
-                    const int q = q0 + __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    int dz = cz - s_rel[q * 3 + 0];
-                    int dy = cy - s_rel[q * 3 + 1];
-                    int dx = cx - s_rel[q * 3 + 2];
-                    if (dz < 0) dz += g.nf[0];
-                    if (dy < 0) dy += g.nf[1];
-                    if (dx < 0) dx += g.nf[2];
-                    const bool in = dz < w0 && dy < w1 && dx < w2;
-                    float wgt = 0.f;
-                    if (in)
-                        wgt = s_w[(q * 3 + 0) * kMaxWidth + dz] * s_w[(q * 3 + 1) * kMaxWidth + dy] *
-                              s_w[(q * 3 + 2) * kMaxWidth + dx];
-                    const float2* vq = s_val + q * CC;
-#pragma unroll
-                    for (int c = 0; c < CC; c += 2) {
-                        if (CC == 1) {
+                        const float2* vq = bval + q * CC;
+                        if constexpr (CC == 1) {
                             const float2 v = vq[0];
                             ar[0] = fmaf(wgt, v.x, ar[0]);
                             ai[0] = fmaf(wgt, v.y, ai[0]);
                         } else {
-                            const float4 v = *reinterpret_cast<const float4*>(vq + c);
-                            ar[c] = fmaf(wgt, v.x, ar[c]);
-                            ai[c] = fmaf(wgt, v.y, ai[c]);
-                            ar[c + 1] = fmaf(wgt, v.z, ar[c + 1]);
-                            ai[c + 1] = fmaf(wgt, v.w, ai[c + 1]);
+#pragma unroll
+                            for (int c = 0; c < CC; c += 2) {
+                                const float4 v = *reinterpret_cast<const float4*>(vq + c);
+                                ar[c] = fmaf(wgt, v.x, ar[c]);
+                                ai[c] = fmaf(wgt, v.y, ai[c]);
+                                ar[c + 1] = fmaf(wgt, v.z, ar[c + 1]);
+                                ai[c + 1] = fmaf(wgt, v.w, ai[c + 1]);
+                            }
                         }
                     }
                 }
             }
+            cp_async_wait_all();
             __syncthreads();
         }
-        // write this cell's transforms
-        if (cz < T0 && cy < T1 && cx < T2) {
-            const int64_t gi = ((int64_t)(o0 + cz) * g.nf[1] + (o1 + cy)) * g.nf[2] + (o2 + cx);
-            float2* dst = a.grid + gi * g.C + cc0;
+        // write the tile: each warp transposes its 32 cells x H coils through shared memory
+        {
+            constexpr int H = SM::kHalf;
+            constexpr int CPR = 32 / H;  // cells per store round
+            float2* ow = reinterpret_cast<float2*>(region) + warp * 32 * (H + 1);
 #pragma unroll
-            for (int c = 0; c < CC; ++c) {
-                if (cc0 + c >= g.C) break;
-                if (extra_mode) {
-                    atomicAdd(&dst[c].x, ar[c]);
-                    atomicAdd(&dst[c].y, ai[c]);
-                } else {
-                    dst[c] = make_float2(ar[c], ai[c]);
+            for (int h0 = 0; h0 < CC; h0 += H) {
+#pragma unroll
+                for (int c = 0; c < H; ++c) ow[lane * (H + 1) + c] = make_float2(ar[h0 + c], ai[h0 + c]);
+                __syncwarp();
+                const int c = lane % H;
+                const int cg = cc0 + h0 + c;
+                for (int j0 = 0; j0 < 32; j0 += CPR) {
+                    const int j = j0 + lane / H;
+                    const int jz = bzi * wb.bz + j / (wb.by * wb.bx);
+                    const int jy = byi * wb.by + (j / wb.bx) % wb.by;
+                    const int jx = bxi * wb.bx + j % wb.bx;
+                    if (cg < g.C) {
+                        const int64_t gi = ((int64_t)(org0 + jz) * nf1 + (org1 + jy)) * nf2 + (org2 + jx);
+                        const float2 v = ow[j * (H + 1) + c];
+                        float2* dst = a.grid + gi * g.C + cg;
+                        if (extra_mode)
+                            atomicAdd(dst, v);
+                        else
+                            *dst = v;
+                    }
                 }
+                __syncwarp();
             }
         }
+        __syncthreads();  // the next coil chunk restages into the region
     }
 }
 
@@ -662,34 +727,42 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
                         // issue the whole W x W slab of gathers before any multiply
                         float2 v[W * W];
 #pragma unroll
-                        for (int dy = 0; dy < W; ++dy)
+                        for (int dy = 0; dy < W; ++dy) {
+                            const float2* rowp = gridc + rowbase[dy];
 #pragma unroll
                             for (int dx = 0; dx < W; ++dx)
-                                v[dy * W + dx] = dy < wy ? gridc[rowbase[dy] + colofs[dx]] : make_float2(0.f, 0.f);
+                                v[dy * W + dx] = dy < wy ? rowp[colofs[dx]] : make_float2(0.f, 0.f);
+                        }
 #pragma unroll
                         for (int dy = 0; dy < W; ++dy) {
-                            const float wzy = dy < wy ? wzv * wts[kMaxWidth + dy] : 0.f;
+                            // row partial sum with the axis-2 weights, then one multiply by the row weight
+                            float rr = 0.f, ri = 0.f;
 #pragma unroll
                             for (int dx = 0; dx < W; ++dx) {
-                                const float wgt = wzy * wx[dx];
-                                ar = fmaf(wgt, v[dy * W + dx].x, ar);
-                                ai = fmaf(wgt, v[dy * W + dx].y, ai);
+                                rr = fmaf(wx[dx], v[dy * W + dx].x, rr);
+                                ri = fmaf(wx[dx], v[dy * W + dx].y, ri);
                             }
+                            const float wzy = dy < wy ? wzv * wts[kMaxWidth + dy] : 0.f;
+                            ar = fmaf(wzy, rr, ar);
+                            ai = fmaf(wzy, ri, ai);
                         }
                     } else {
 #pragma unroll
                         for (int dy = 0; dy < W; ++dy) {
                             if (dy < wy) {
                                 const float wzy = wzv * wts[kMaxWidth + dy];
+                                const float2* rowp = gridc + rowbase[dy];
                                 float2 v[W];
 #pragma unroll
-                                for (int dx = 0; dx < W; ++dx) v[dx] = gridc[rowbase[dy] + colofs[dx]];
+                                for (int dx = 0; dx < W; ++dx) v[dx] = rowp[colofs[dx]];
+                                float rr = 0.f, ri = 0.f;
 #pragma unroll
                                 for (int dx = 0; dx < W; ++dx) {
-                                    const float wgt = wzy * wx[dx];
-                                    ar = fmaf(wgt, v[dx].x, ar);
-                                    ai = fmaf(wgt, v[dx].y, ai);
+                                    rr = fmaf(wx[dx], v[dx].x, rr);
+                                    ri = fmaf(wx[dx], v[dx].y, ri);
                                 }
+                                ar = fmaf(wzy, rr, ar);
+                                ai = fmaf(wzy, ri, ai);
                             }
                         }
                     }
@@ -1158,17 +1231,16 @@ static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t 
     if (cells == 512 && g.dim >= 2) {
         // output-stationary kernel: one thread per cell of an 8x8x8 (3-D) or 16x32 (2-D) tile
         SpreadTileShape wb{p->wb[0], p->wb[1], p->wb[2]};
-        const size_t smem = sizeof(float) * (kCoefFloats + (size_t)kSpreadChunk * 3 * kMaxWidth) +
-                            sizeof(float2) * (size_t)kSpreadChunk * CC + sizeof(int) * kSpreadChunk * 8;
+        const size_t smem = sizeof(float) * (size_t)SpreadSmem<CC>::kFloats;
         HB_CUDA(cudaFuncSetAttribute(k_spread_reg<CC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         {
             TimedSection ts("spread", s);
-            k_spread_reg<CC><<<(unsigned)p->nbins, 512, smem, s>>>(a, 0, wb);
+            k_spread_reg<CC><<<(unsigned)p->nbins, kSpreadThreads, smem, s>>>(a, 0, wb);
             HB_TRY(check_launch("k_spread_reg"));
         }
         if (p->n_extra > 0) {
             TimedSection ts("spread_dense", s);
-            k_spread_reg<CC><<<(unsigned)p->n_extra, 512, smem, s>>>(a, 1, wb);
+            k_spread_reg<CC><<<(unsigned)p->n_extra, kSpreadThreads, smem, s>>>(a, 1, wb);
             HB_TRY(check_launch("k_spread_reg(extra)"));
         }
         return HB_OK;
