@@ -4,7 +4,7 @@ given problem by timing type-1 plans on the device, and caches the choice as JSO
 Search space (all exact, all give the same result up to float rounding):
 - the 32-cell block each warp owns inside a spread tile: 3-D tiles are 8x8x8, so any
   (bz, by, bx) with bz*by*bx = 32 and each edge dividing 8; 2-D tiles are 16x32;
-- points per subproblem (how dense tiles are split across CTAs): 512 .. 4096.
+- points per subproblem (how dense tiles are split across CTAs): 1024 .. 8192.
 
 Cache key: dimensionality, modes, transforms, kernel width, number of points and a coarse
 density signature of the trajectory (quartiles of |k|), so the same trajectory family reuses the
@@ -23,7 +23,7 @@ from .nufft import NufftOpts, NufftPlan, NufftType
 
 BLOCKS_3D = [(2, 4, 4), (4, 4, 2), (2, 2, 8), (4, 2, 4), (1, 4, 8), (8, 2, 2), (2, 8, 2)]
 BLOCKS_2D = [(1, 4, 8), (1, 8, 4), (1, 2, 16), (1, 16, 2), (1, 1, 32)]
-MAXP = [512, 1024, 2048, 4096]
+MAXP = [1024, 2048, 4096, 8192]
 
 
 def cache_path() -> Path:

@@ -498,8 +498,15 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
     const float hw = a.kb.hw;
     const bool vec = (g.C % 2) == 0;
 
-    // candidate k of this tile -> sorted point index
-    auto sorted_index = [&](int k) -> int {
+    // Candidate k of this tile -> sorted point index. The candidates are visited interleaved:
+    // the list (bins concatenated) is cut into 8 near-equal segments and k takes segment k % 8,
+    // position k / 8, so every chunk samples all of the tile's bins and the warps' shares of a
+    // chunk stay even (a chunk drawn from one lower-neighbour bin would only reach the warps at
+    // the tile's low faces).
+    const int seg_len = total >> 3, seg_rem = total & 7;
+    auto sorted_index = [&](int k0) -> int {
+        const int sg = k0 & 7;
+        const int k = sg * seg_len + min(sg, seg_rem) + (k0 >> 3);
         int b = 0;
 #pragma unroll
         for (int j = 1; j < 8; ++j) b += (j < nbin && s_pref[j] <= k) ? 1 : 0;

@@ -55,7 +55,7 @@ struct NufftPlan {
     int* d_err = nullptr;
     bool pts_set = false;
     // spreading knobs (autotuned): candidates per subproblem and the warp's cell block
-    int maxp = 1024;
+    int maxp = 4096;
     int wb[3] = {2, 4, 4};
     size_t device_bytes = 0;
 };

@@ -151,7 +151,7 @@ class NufftPlan:
             pass
 
     # -- extras ----------------------------------------------------------------------------------
-    def set_spread_tuning(self, max_candidates: int = 1024, block=(2, 4, 4)) -> None:
+    def set_spread_tuning(self, max_candidates: int = 4096, block=(2, 4, 4)) -> None:
         """Spreading knobs (before setpts): points per subproblem and the warp's cell block
         (image order; 2-D plans take (1, by, bx))."""
         if self.M is not None:
