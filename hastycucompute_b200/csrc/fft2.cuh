@@ -14,6 +14,8 @@
 // x[n2 + Q n1].
 #pragma once
 
+#include <type_traits>
+
 #include "fft.cuh"
 
 namespace hb {
@@ -121,18 +123,36 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 //       multiplies by kptr(kcol(e))[pos]; the CTA stages its distinct columns in shared memory)
 //   const float2* srow(int64_t a, int64_t e) const                      (kSenseReduce: the
 //       factor row of (a, e), staged per chunk; product_s(v, s) combines a value with it)
-template <int P, int Q, class Op>
+//
+// HM (compile-time pass shape): bit 0 = the input is zero-padded to twice its length at offset 0
+// (Lin == L/2, in_shift == 0), so only samples j < P/2 of step 1 are loaded and the P-point DFT
+// skips the zero half; bit 1 = the output is the first half (Lout == L/2, out_shift == 0), so
+// step 2 stores k2 < Q/2 (fused passes: step 3 stores n1 < P/2) with no position checks.
+template <int P, int Q, class Op, int HM = 0>
 __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduce ? 2 : 3)) pass2_kernel(const Op op, const PassCfg c) {
     constexpr int L = P * Q;
     constexpr int CWp = kCW + 1;
+    constexpr bool kHalfIn = (HM & 1) != 0;
+    constexpr bool kHalfOut = (HM & 2) != 0;
+    static_assert(!kHalfIn || P % 2 == 0, "half input needs an even P");
+    static_assert(!kHalfOut || (P % 2 == 0 && Q % 2 == 0), "half output needs even P and Q");
     extern __shared__ float2 smem2[];
-    float2* tw = smem2;       // L
-    float2* Y = smem2 + L;    // [L][CWp] transpose buffer
+    // Outer twiddles from a [Q][P] table: one base address per thread and constant offsets.
+    // Step 1 uses it when a warp spans few rows t (column-fast loads); with row-fast loads the
+    // lanes' rows are P entries apart and would collide in the shared banks, so those passes
+    // index tw[t * k1]. Fused passes also read it in step 2, by column.
+    constexpr bool kT2 = Op::kFusedK || !Op::kLoadLFast;
+    float2* tw = smem2;                // L: tw[m] = W_L^m
+    float2* T2 = tw + L;               // kT2: [Q][P], T2[t * P + k1] = W_L^(t k1)
+    float2* Y = T2 + (kT2 ? L : 0);    // [L][CWp] transpose buffer
     float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][groups][Lout] running sums
     float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * op.ngroups() * c.Lout : 0);  // kFusedK: [kMaxKCols][L]
     float2* Ss = Ks + (Op::kFusedK ? kMaxKCols * L : 0);          // kSenseReduce: [W][Lout]
 
-    for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = c.tw[i];
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        tw[i] = c.tw[i];
+        if constexpr (kT2) T2[i] = c.tw[(i / P) * (i % P)];  // (Q-1)(P-1) < L
+    }
     if constexpr (Op::kSenseReduce)
         for (int i = threadIdx.x; i < c.A_blk * op.ngroups() * c.Lout; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
 
@@ -190,29 +210,40 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             const int64_t a = a0 + al, e = e0 + el;
             const bool colok = col < c.W && a < c.A && e < c.E;
             float2 v[P];
+            bool halfzero;
+            if constexpr (kHalfIn) {
 #pragma unroll
-            for (int j = 0; j < P; ++j) {
-                const int pos = t + Q * j;
-                int l = pos - in_shift;
-                if (l < 0) l += L;
-                v[j] = (colok && l < c.Lin) ? op.load(a, l, e) : make_float2(0.f, 0.f);
+                for (int j = 0; j < P; ++j)
+                    v[j] = (j < P / 2 && colok) ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
+                halfzero = true;
+            } else {
+#pragma unroll
+                for (int j = 0; j < P; ++j) {
+                    const int pos = t + Q * j;
+                    int l = pos - in_shift;
+                    if (l < 0) l += L;
+                    v[j] = (colok && l < c.Lin) ? op.load(a, l, e) : make_float2(0.f, 0.f);
+                }
+                // zero padding to 2x (Lin == L/2 at shift 0): only v[0..P/2) can be non-zero
+                halfzero = (2 * c.Lin == L) && in_shift == 0;
             }
-            // zero padding to 2x (Lin == L/2 at shift 0): only v[0..P/2) can be non-zero
-            const bool halfzero = (2 * c.Lin == L) && in_shift == 0;
+            // W_L^(t k1) = trow[k1 * tstep]
+            const float2* trow = (kT2 && !Op::kLoadLFast) ? T2 + t * P : tw;
+            const int tstep = (kT2 && !Op::kLoadLFast) ? 1 : t;
             if (c.inverse) {
                 if (halfzero)
                     dft_reg_halfzero<P, true>(v, tw, Q);
                 else
                     dft_reg<P, true>(v, tw, Q);
 #pragma unroll
-                for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<true>(tw, t * k1));
+                for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<true>(trow, k1 * tstep));
             } else {
                 if (halfzero)
                     dft_reg_halfzero<P, false>(v, tw, Q);
                 else
                     dft_reg<P, false>(v, tw, Q);
 #pragma unroll
-                for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<false>(tw, t * k1));
+                for (int k1 = 1; k1 < P; ++k1) v[k1] = cmul(v[k1], tw_get<false>(trow, k1 * tstep));
             }
 #pragma unroll
             for (int k1 = 0; k1 < P; ++k1) Y[(k1 * Q + t) * CWp + col] = v[k1];
@@ -253,14 +284,15 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
 #pragma unroll
                     for (int k2 = 0; k2 < Q; ++k2) u[k2] = colok2 ? cmul(u[k2], op.kval(a2, k1 + P * k2, e2)) : make_float2(0.f, 0.f);
                 }
+                const float2* tcol = T2 + k1;  // W_L^(n2 k1) = tcol[n2 * P]
                 if (c.inverse) {
                     dft_reg<Q, false>(u, tw, P);
 #pragma unroll
-                    for (int n2 = 1; n2 < Q; ++n2) u[n2] = cmul(u[n2], tw_get<false>(tw, n2 * k1));
+                    for (int n2 = 1; n2 < Q; ++n2) u[n2] = cmul(u[n2], tw_get<false>(tcol, n2 * P));
                 } else {
                     dft_reg<Q, true>(u, tw, P);
 #pragma unroll
-                    for (int n2 = 1; n2 < Q; ++n2) u[n2] = cmul(u[n2], tw_get<true>(tw, n2 * k1));
+                    for (int n2 = 1; n2 < Q; ++n2) u[n2] = cmul(u[n2], tw_get<true>(tcol, n2 * P));
                 }
 #pragma unroll
                 for (int n2 = 0; n2 < Q; ++n2) Y[(k1 * Q + n2) * CWp + col2] = u[n2];
@@ -280,12 +312,17 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
                 else
                     dft_reg<P, true>(z, tw, Q);
                 if (colok3) {
+                    if constexpr (kHalfOut) {
 #pragma unroll
-                    for (int n1 = 0; n1 < P; ++n1) {
-                        const int pos = n2 + Q * n1;
-                        int o = pos - out_shift;
-                        if (o < 0) o += L;
-                        if (o < c.Lout) op.store(a3, o, e3, z[n1]);
+                        for (int n1 = 0; n1 < P / 2; ++n1) op.store(a3, n2 + Q * n1, e3, z[n1]);
+                    } else {
+#pragma unroll
+                        for (int n1 = 0; n1 < P; ++n1) {
+                            const int pos = n2 + Q * n1;
+                            int o = pos - out_shift;
+                            if (o < 0) o += L;
+                            if (o < c.Lout) op.store(a3, o, e3, z[n1]);
+                        }
                     }
                 }
             }
@@ -293,12 +330,17 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             // spectra into Y[o][col]; then thread o forms sum_col product(v) for its row
             __syncthreads();  // everyone has read Y
             if (s2active) {
+                if constexpr (kHalfOut) {
 #pragma unroll
-                for (int k2 = 0; k2 < Q; ++k2) {
-                    const int pos = k1 + P * k2;
-                    int o = pos - out_shift;
-                    if (o < 0) o += L;
-                    if (o < c.Lout) Y[o * CWp + col2] = u[k2];
+                    for (int k2 = 0; k2 < Q / 2; ++k2) Y[(k1 + P * k2) * CWp + col2] = u[k2];
+                } else {
+#pragma unroll
+                    for (int k2 = 0; k2 < Q; ++k2) {
+                        const int pos = k1 + P * k2;
+                        int o = pos - out_shift;
+                        if (o < 0) o += L;
+                        if (o < c.Lout) Y[o * CWp + col2] = u[k2];
+                    }
                 }
             }
             __syncthreads();
@@ -342,12 +384,17 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             }
         } else {
             if (colok2) {
+                if constexpr (kHalfOut) {
 #pragma unroll
-                for (int k2 = 0; k2 < Q; ++k2) {
-                    const int pos = k1 + P * k2;
-                    int o = pos - out_shift;
-                    if (o < 0) o += L;
-                    if (o < c.Lout) op.store(a2, o, e2, u[k2]);
+                    for (int k2 = 0; k2 < Q / 2; ++k2) op.store(a2, k1 + P * k2, e2, u[k2]);
+                } else {
+#pragma unroll
+                    for (int k2 = 0; k2 < Q; ++k2) {
+                        const int pos = k1 + P * k2;
+                        int o = pos - out_shift;
+                        if (o < 0) o += L;
+                        if (o < c.Lout) op.store(a2, o, e2, u[k2]);
+                    }
                 }
             }
         }
@@ -378,16 +425,36 @@ inline void reg_split(int L, int* P, int* Q) {
     }
 }
 
+// Op::kHalfIO (optional, default 0): the HM shape every pass of this operator has.
+template <class Op, class = void>
+struct HalfIO {
+    static constexpr int value = 0;
+};
+template <class Op>
+struct HalfIO<Op, std::void_t<decltype(Op::kHalfIO)>> {
+    static constexpr int value = Op::kHalfIO;
+};
+
 template <int P, int Q, class Op>
 int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s, const char* name) {
     constexpr int L = P * Q;
-    size_t smem = (size_t)(L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
+    constexpr int HM = HalfIO<Op>::value;
+    if constexpr (HM != 0) {
+        const int in_sh = ((c.in_shift % L) + L) % L, out_sh = ((c.out_shift % L) + L) % L;
+        const bool ok_in = !(HM & 1) || (2 * c.Lin == L && in_sh == 0);
+        const bool ok_out = !(HM & 2) || (2 * c.Lout == L && out_sh == 0);
+        if (!ok_in || !ok_out) {
+            set_error(std::string(name) + ": pass shape does not match the operator's padding / crop");
+            return HB_ERR_INVALID_ARG;
+        }
+    }
+    size_t smem = (size_t)((Op::kFusedK || !Op::kLoadLFast ? 2 : 1) * L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
     if (Op::kFusedK) smem += (size_t)kMaxKCols * L * sizeof(float2);
     if (Op::kSenseReduce) smem += (size_t)c.W * c.Lout * sizeof(float2);
-    cudaError_t e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op, HM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // the staging passes want every CTA they can fit; plain passes keep the default L1 split
     if (e == cudaSuccess && (Op::kFusedK || Op::kSenseReduce))
-        e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op, HM>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) {
         set_error(std::string(name) + ": cudaFuncSetAttribute failed: " + cudaGetErrorString(e));
@@ -401,7 +468,7 @@ int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s,
         return HB_ERR_INVALID_ARG;
     }
     TimedSection ts(name, s);
-    pass2_kernel<P, Q, Op><<<(unsigned)blocks, Q * kCW, smem, s>>>(op, c);
+    pass2_kernel<P, Q, Op, HM><<<(unsigned)blocks, Q * kCW, smem, s>>>(op, c);
     return check_launch(name);
 }
 

@@ -90,6 +90,7 @@ static int get_len(int L, FftLen* out) {
 #ifdef __CUDACC__
 
 struct OpToepIn {
+    static constexpr int kHalfIO = 1;  // pass shape (pass2_kernel HM)
     static constexpr bool kLoadLFast = true;
     static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = false;
@@ -131,8 +132,18 @@ struct OpToepIn {
     __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
 };
 
+// The Toeplitz passes along the middle axis: zero-padding N -> 2N (forward) and cropping
+// 2N -> N (inverse), both at offset 0.
+struct OpStridedPad : OpStrided {
+    static constexpr int kHalfIO = 1;
+};
+struct OpStridedCrop : OpStrided {
+    static constexpr int kHalfIO = 2;
+};
+
 // In-place fused pass: FFT, * Kt[col][pos], IFFT, crop. buf[l][e] with row stride E.
 struct OpToepMid {
+    static constexpr int kHalfIO = 3;  // pass shape (pass2_kernel HM)
     static constexpr bool kLoadLFast = false;
     static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = true;
@@ -163,6 +174,7 @@ struct OpToepMid {
 };
 
 struct OpToepOutFlat {
+    static constexpr int kHalfIO = 2;  // pass shape (pass2_kernel HM)
     static constexpr bool kLoadLFast = false;
     static constexpr bool kStoreLFast = true;
     static constexpr bool kFusedK = false;
@@ -206,6 +218,7 @@ struct OpToepOutFlat {
 // columns e = f * cpf + c (one frame when cpf = B). The CTA walks every batch chunk of its rows and
 // keeps one running sum per (row, frame) in shared memory (extra).
 struct OpToepOutSense {
+    static constexpr int kHalfIO = 2;  // pass shape (pass2_kernel HM)
     static constexpr bool kLoadLFast = false;
     static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = false;
@@ -278,8 +291,24 @@ struct OpToepOutSense {
     }
 };
 
-// Kt[(c)*L + z] = K[z][c] * scale : transpose [R][Ccols] -> [Ccols][R]
-__global__ void k_transpose_scale(const float2* __restrict__ in, float2* __restrict__ out, int64_t R, int64_t Cc, float scale) {
+// The crop of the straight convolution keeps positions [N-1, 2N-1) of each axis. A circular shift
+// of the inverse transform's output by s = N - 1 is a phase ramp on its input,
+//     y[i + s] = sum_k (K[k] exp(+2 pi i k s / L)) X[k] exp(+2 pi i k i / L),
+// so the transformed kernel carries the ramp of every axis and all passes crop at offset 0.
+// (kr, kc) index the kernel as [R][Cc] with Cc = Lb * Lc (3-D) or Lb (2-D, Lc = 1).
+__device__ __forceinline__ float2 crop_ramp(float2 v, int64_t kr, int64_t kc, int64_t R, int64_t Lb, int64_t Lc) {
+    const int64_t kb = kc / Lc, kk = kc % Lc;
+    double ph = 2.0 * ((double)((kr * (R / 2 - 1)) % R) / (double)R + (double)((kb * (Lb / 2 - 1)) % Lb) / (double)Lb);
+    if (Lc > 1) ph += 2.0 * (double)((kk * (Lc / 2 - 1)) % Lc) / (double)Lc;
+    ph -= 2.0 * floor(ph * 0.5);  // radians / pi in [0, 2)
+    double sn, cs;
+    sincospi(ph, &sn, &cs);
+    return make_float2((float)((double)v.x * cs - (double)v.y * sn), (float)((double)v.x * sn + (double)v.y * cs));
+}
+
+// Kt[c * R + z] = K[z][c] * scale * ramp : transpose [R][Cc] -> [Cc][R]
+__global__ void k_transpose_scale(const float2* __restrict__ in, float2* __restrict__ out, int64_t R, int64_t Cc,
+                                  int64_t Lb, int64_t Lc, float scale) {
     __shared__ float2 tile[32][33];
     const int64_t c0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
     for (int j = threadIdx.y; j < 32; j += blockDim.y) {
@@ -289,7 +318,7 @@ __global__ void k_transpose_scale(const float2* __restrict__ in, float2* __restr
     __syncthreads();
     for (int j = threadIdx.y; j < 32; j += blockDim.y) {
         const int64_t c = c0 + j, r = r0 + threadIdx.x;
-        if (r < R && c < Cc) out[c * R + r] = cscale(tile[threadIdx.x][j], scale);
+        if (r < R && c < Cc) out[c * R + r] = crop_ramp(cscale(tile[threadIdx.x][j], scale), r, c, R, Lb, Lc);
     }
 }
 
@@ -328,35 +357,35 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
     if (t.dim == 3) {
         // P2: axis 1, pad N1 -> L1, forward
         {
-            OpStrided op{W1, W2, N1 * E2, E2, (int64_t)L1 * E2, E2, 1.0f};
+            OpStridedPad op{{W1, W2, N1 * E2, E2, (int64_t)L1 * E2, E2, 1.0f}};
             HB_TRY(launch_fft_pass(op, f1, N0, E2, (int)N1, 0, L1, 0, 0, 0, s, "toeplitz P2"));
         }
         // P3: axis 0 fused, in place on W2
         {
             const int64_t E = (int64_t)L1 * E2;
             OpToepMid op{W2, a.kt, E, a.frames > 1 ? cpf : B, L0};
-            HB_TRY(launch_fft_pass(op, f0, 1, E, (int)N0, 0, (int)N0, (int)(N0 - 1), 0, 0, s, "toeplitz P3"));
+            HB_TRY(launch_fft_pass(op, f0, 1, E, (int)N0, 0, (int)N0, 0, 0, 0, s, "toeplitz P3"));
         }
         // P4: axis 1 inverse, crop -> W1
         {
-            OpStrided op{W2, W1, (int64_t)L1 * E2, E2, N1 * E2, E2, 1.0f};
-            HB_TRY(launch_fft_pass(op, f1, N0, E2, L1, 0, (int)N1, (int)(N1 - 1), 1, 0, s, "toeplitz P4"));
+            OpStridedCrop op{{W2, W1, (int64_t)L1 * E2, E2, N1 * E2, E2, 1.0f}};
+            HB_TRY(launch_fft_pass(op, f1, N0, E2, L1, 0, (int)N1, 0, 1, 0, s, "toeplitz P4"));
         }
     } else {
         // fused pass along axis 1, in place on W1 ([1][N1][L2][B])
         OpToepMid op{W1, a.kt, E2, a.frames > 1 ? cpf : B, L1};
-        HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0, 0, s, "toeplitz P3"));
+        HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, 0, 0, 0, s, "toeplitz P3"));
     }
     // P5: axis 2 inverse, crop, output ops
     {
         if (a.sense) {
             OpToepOutSense op{W1, (int64_t)L2 * B, B, a.in, a.out, N2, t.n, cpf, (int)a.frames};
-            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1,
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, 0, 1,
                                    sizeof(float2) * (size_t)N2 * a.frames, s, "toeplitz P5 sense"));
         } else {
             OpToepOutFlat op{W1, (int64_t)L2 * B, B, a.in, a.m1, a.m2, a.io_mult, a.out_m1, a.out_m2, a.accumulate,
                              a.out, N2, t.n};
-            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1, 0, s, "toeplitz P5"));
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, 0, 1, 0, s, "toeplitz P5"));
         }
     }
     return HB_OK;
@@ -478,7 +507,7 @@ int sense_normal_batched(int dim, const int64_t* shape, int64_t nframes, int64_t
 
 // Kt[(c * F + f) * R + r] = K_f[r][c] * scale : per-frame transpose [F][R][Cc] -> [Cc][F][R]
 __global__ void k_transpose_scale_frames(const float2* __restrict__ in, float2* __restrict__ out, int64_t R, int64_t Cc,
-                                         int64_t F, float scale) {
+                                         int64_t Lb, int64_t Lc, int64_t F, float scale) {
     __shared__ float2 tile[32][33];
     const int64_t f = blockIdx.z;
     const int64_t c0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
@@ -490,7 +519,7 @@ __global__ void k_transpose_scale_frames(const float2* __restrict__ in, float2* 
     __syncthreads();
     for (int j = threadIdx.y; j < 32; j += blockDim.y) {
         const int64_t c = c0 + j, r = r0 + threadIdx.x;
-        if (r < R && c < Cc) out[(c * F + f) * R + r] = cscale(tile[threadIdx.x][j], scale);
+        if (r < R && c < Cc) out[(c * F + f) * R + r] = crop_ramp(cscale(tile[threadIdx.x][j], scale), r, c, R, Lb, Lc);
     }
 }
 
@@ -507,7 +536,8 @@ int transform_toeplitz_kernels(int dim, const int64_t* kshape, int64_t nframes, 
     }
     const float scale = (float)(1.0 / (double)tot);
     dim3 grid((unsigned)ceil_div(Cc, 32), (unsigned)ceil_div(R, 32), (unsigned)nframes);
-    k_transpose_scale_frames<<<grid, dim3(32, 8), 0, s>>>((const float2*)kin, (float2*)kout, R, Cc, nframes, scale);
+    const int64_t Lb = kshape[1], Lc = dim == 3 ? kshape[2] : 1;
+    k_transpose_scale_frames<<<grid, dim3(32, 8), 0, s>>>((const float2*)kin, (float2*)kout, R, Cc, Lb, Lc, nframes, scale);
     return check_launch("transform_toeplitz_kernels");
 }
 
@@ -523,7 +553,8 @@ int transform_toeplitz_kernel(int dim, const int64_t* kshape, const void* kin, v
     }
     const float scale = (float)(1.0 / (double)tot);
     dim3 grid((unsigned)ceil_div(Cc, 32), (unsigned)ceil_div(R, 32));
-    k_transpose_scale<<<grid, dim3(32, 8), 0, s>>>((const float2*)kin, (float2*)kout, R, Cc, scale);
+    const int64_t Lb = kshape[1], Lc = dim == 3 ? kshape[2] : 1;
+    k_transpose_scale<<<grid, dim3(32, 8), 0, s>>>((const float2*)kin, (float2*)kout, R, Cc, Lb, Lc, scale);
     return check_launch("transform_toeplitz_kernel");
 }
 
@@ -698,25 +729,25 @@ int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const vo
     }
     if (t.dim == 3) {
         {
-            OpStrided op{W1, W2, N1 * E2, E2, (int64_t)L1 * E2, E2, 1.0f};
+            OpStridedPad op{{W1, W2, N1 * E2, E2, (int64_t)L1 * E2, E2, 1.0f}};
             HB_TRY(launch_fft_pass(op, f1, N0, E2, (int)N1, 0, L1, 0, 0, 0, s, "noalloc P2"));
         }
         {
             const int64_t E = (int64_t)L1 * E2;
             OpToepMid op{W2, (const float2*)kernel, E, B, L0};
-            HB_TRY(launch_fft_pass(op, f0, 1, E, (int)N0, 0, (int)N0, (int)(N0 - 1), 0, 0, s, "noalloc P3"));
+            HB_TRY(launch_fft_pass(op, f0, 1, E, (int)N0, 0, (int)N0, 0, 0, 0, s, "noalloc P3"));
         }
         {
-            OpStrided op{W2, W1, (int64_t)L1 * E2, E2, N1 * E2, E2, 1.0f};
-            HB_TRY(launch_fft_pass(op, f1, N0, E2, L1, 0, (int)N1, (int)(N1 - 1), 1, 0, s, "noalloc P4"));
+            OpStridedCrop op{{W2, W1, (int64_t)L1 * E2, E2, N1 * E2, E2, 1.0f}};
+            HB_TRY(launch_fft_pass(op, f1, N0, E2, L1, 0, (int)N1, 0, 1, 0, s, "noalloc P4"));
         }
     } else {
         OpToepMid op{W1, (const float2*)kernel, E2, B, L1};
-        HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, (int)(N1 - 1), 0, 0, s, "noalloc P3"));
+        HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, 0, 0, 0, s, "noalloc P3"));
     }
     {
         OpToepOutSense op{W1, E2, B, S, (float2*)out, N2, t.n, B, 1};
-        HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, (int)(N2 - 1), 1, sizeof(float2) * (size_t)N2, s,
+        HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, 0, 1, sizeof(float2) * (size_t)N2, s,
                                "noalloc P5 sense"));
     }
     return HB_OK;

@@ -135,7 +135,9 @@ int hb_toeplitz_kernel(int dim, const int64_t* kernel_shape, int64_t M, const fl
 /* transform_toeplitz_kernel, cpp/corelib/lib/fft/toeplitz.cppm:510-609: re-lays the
  * straight kernel ([2N..] c64, from hb_toeplitz_kernel) into the layout
  * hb_toeplitz_multiplication / hb_sense_normal read (same element count, c64), with the
- * inverse-FFT normalisation 1/prod(2N) folded in. in and out must not alias. */
+ * inverse-FFT normalisation 1/prod(2N) and, per axis, the phase ramp exp(+2 pi i k (N-1) / 2N)
+ * folded in (it moves the crop [N-1, 2N-1) of the inverse transform to [0, N)). in and out must
+ * not alias. */
 int hb_transform_toeplitz_kernel(int dim, const int64_t* kernel_shape, const void* kernel_in,
                                  void* kernel_out, void* stream);
 
