@@ -153,8 +153,10 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
         tw[i] = c.tw[i];
         if constexpr (kT2) T2[i] = c.tw[(i / P) * (i % P)];  // (Q-1)(P-1) < L
     }
-    if constexpr (Op::kSenseReduce)
-        for (int i = threadIdx.x; i < c.A_blk * op.ngroups() * c.Lout; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+    const int tid = threadIdx.x;
+    const int in_shift = ((c.in_shift % L) + L) % L;
+    const int out_shift = ((c.out_shift % L) + L) % L;
+    __syncthreads();
 
     int64_t ab, eb_begin, eb_end;
     if (Op::kChunkLoop) {
@@ -167,10 +169,10 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
         eb_end = eb_begin + 1;
     }
     const int64_t a0 = ab * c.A_blk;
-    const int tid = threadIdx.x;
-    const int in_shift = ((c.in_shift % L) + L) % L;
-    const int out_shift = ((c.out_shift % L) + L) % L;
-    __syncthreads();
+    if constexpr (Op::kSenseReduce) {
+        for (int i = tid; i < c.A_blk * op.ngroups() * c.Lout; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+        __syncthreads();
+    }
 
     for (int64_t eb = eb_begin; eb < eb_end; ++eb) {
         const int64_t e0 = eb * c.E_blk;
@@ -188,11 +190,19 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             }
         }
         if constexpr (Op::kSenseReduce) {
-            for (int i = tid; i < c.W * c.Lout; i += blockDim.x) {
-                const int col = i / c.Lout, o = i % c.Lout;
-                const int al = col / c.E_blk, el = col % c.E_blk;
+            // one warp per column row: the row pointer once, then contiguous copies
+            const int lane = tid & 31, nw = blockDim.x >> 5;
+            for (int col = tid >> 5; col < c.W; col += nw) {
+                const int al = col / c.E_blk, el = col - al * c.E_blk;
                 const int64_t a = a0 + al, e = e0 + el;
-                if (a < c.A && e < c.E) cp_async8(Ss + i, op.srow(a, e) + o);
+                if (a >= c.A || e >= c.E) continue;
+                const float2* src = op.srow(a, e);
+                float2* dst = Ss + col * c.Lout;
+                if ((((uintptr_t)src | (uintptr_t)dst) & 15) == 0 && (c.Lout & 1) == 0) {
+                    for (int o = 2 * lane; o < c.Lout; o += 64) cp_async16(dst + o, src + o);
+                } else {
+                    for (int o = lane; o < c.Lout; o += 32) cp_async8(dst + o, src + o);
+                }
             }
             cp_async_commit();
         }
@@ -273,8 +283,10 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
                 dft_reg<Q, false>(u, tw, P);
         }
         if constexpr (Op::kFusedK) {
-            // multiply by the kernel at position k1 + P k2, inverse Q-point DFT over k2
-            __syncthreads();  // everyone has read Y
+            // multiply by the kernel at position k1 + P k2, inverse Q-point DFT over k2. The thread
+            // writes back into the transpose slots it read; the barrier is kept as a scheduling
+            // fence (without it the compiler interleaves the two halves and spills).
+            __syncthreads();
             if (s2active) {
                 if (k_staged) {
                     const float2* kc = Ks + (int)(op.kcol(e2) - kc0) * L;
@@ -344,19 +356,19 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
                 }
             }
             __syncthreads();
-            const int tot = c.A_blk * c.Lout;
+            const int Lo = kHalfOut ? L / 2 : c.Lout;
+            const int tot = c.A_blk * Lo;
             const int ng = op.ngroups();
             if (ng == 1) {
                 // one frame: every column of the chunk adds into the row's single sum
+                const int ecount = (int)min((int64_t)c.E_blk, c.E - e0);
                 for (int idx = tid; idx < tot; idx += blockDim.x) {
-                    const int o = idx % c.Lout, al = idx / c.Lout;
+                    const int o = idx % Lo, al = idx / Lo;
                     if (a0 + al >= c.A) continue;
-                    const int ecount = (int)min((int64_t)c.E_blk, c.E - e0);
                     float2 run = acc[idx];
-                    for (int el = 0; el < ecount; ++el) {
-                        const int col = al * c.E_blk + el;
-                        run = cadd(run, op.product_s(Y[o * CWp + col], Ss[col * c.Lout + o]));
-                    }
+                    const float2* yr = Y + o * CWp + al * c.E_blk;
+                    const float2* sr = Ss + (al * c.E_blk) * Lo + o;
+                    for (int el = 0; el < ecount; ++el) run = cadd(run, op.product_s(yr[el], sr[el * Lo]));
                     acc[idx] = run;
                 }
             } else
@@ -398,7 +410,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
                 }
             }
         }
-        __syncthreads();
+        if (eb + 1 < eb_end) __syncthreads();  // the next chunk rewrites Y (and the staged rows)
     }
     if constexpr (Op::kSenseReduce) {
         __syncthreads();

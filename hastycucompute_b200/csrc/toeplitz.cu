@@ -5,11 +5,13 @@
 // one buffer ([..][B], B fastest), a 3-D apply is five pruned passes:
 //   P1 axis 2: load in[b] * mults (N2 samples) -> FFT 2N2            -> W1[N0][N1][2N2][B]
 //   P2 axis 1: N1 samples -> FFT 2N1                                 -> W2[N0][2N1][2N2][B]
-//   P3 axis 0: N0 samples -> FFT 2N0, * K, IFFT 2N0, keep [N0-1,2N0-1) -> W2 (in place)
-//   P4 axis 1: IFFT 2N1, keep [N1-1, 2N1-1)                          -> W1[N0][N1][2N2][B]
-//   P5 axis 2: IFFT 2N2, keep [N2-1, 2N2-1), * output mults (and for SENSE: sum over b of
+//   P3 axis 0: N0 samples -> FFT 2N0, * K, IFFT 2N0, keep [0, N0)      -> W2 (in place)
+//   P4 axis 1: IFFT 2N1, keep [0, N1)                                -> W1[N0][N1][2N2][B]
+//   P5 axis 2: IFFT 2N2, keep [0, N2), * output mults (and for SENSE: sum over b of
 //              conj(S_b) * v inside the CTA)                          -> out
-// A 2-D apply is P1, the fused pass along axis 1, and P5.
+// A 2-D apply is P1, the fused pass along axis 1, and P5. The straight convolution keeps
+// [N-1, 2N-1) of each axis; the transformed kernel carries that shift as a phase ramp, so every
+// pass pads and crops at offset 0 and runs the compile-time pass shapes of pass2_kernel.
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -130,6 +132,17 @@ struct OpToepIn {
         for_each_output<false>(res, c, a0, e0, [&](int64_t a, int o, int64_t e, float2 v) { d[a * da + (int64_t)o * dl + e] = v; });
     }
     __device__ __forceinline__ void finish(const PassCfg&, int64_t, float2*) const {}
+};
+
+// P1 of the SENSE normal operator: column e = f * cpf + c reads S_c[idx] * x_f[idx] (cpf = 0: one
+// frame, x shared by all coils). The product is fixed at compile time.
+struct OpToepInSense : OpToepIn {
+    __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
+        const int64_t idx = a * N2 + l;
+        const int64_t ei = cpf ? e % cpf : e;
+        const int64_t m1o = cpf ? (e / cpf) * n : 0;
+        return cmul(in[ei * n + idx], m1[m1o + idx]);
+    }
 };
 
 // The Toeplitz passes along the middle axis: zero-padding N -> 2N (forward) and cropping
@@ -350,8 +363,14 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
     const int64_t cpf = a.sense ? B / a.frames : 0;  // coils per frame (SENSE)
     // P1: axis 2, pad N2 -> L2, forward
     {
-        OpToepIn op{a.in, a.m1, a.m2, a.in_m1, a.in_m2, W1, N2, t.n, (int64_t)L2 * B, B, a.frames > 1 ? cpf : 0};
-        HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "toeplitz P1"));
+        if (a.sense) {
+            OpToepInSense op{{a.in, a.m1, nullptr, HB_MULT_MULT, HB_MULT_NONE, W1, N2, t.n, (int64_t)L2 * B, B,
+                              a.frames > 1 ? cpf : 0}};
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "toeplitz P1"));
+        } else {
+            OpToepIn op{a.in, a.m1, a.m2, a.in_m1, a.in_m2, W1, N2, t.n, (int64_t)L2 * B, B, a.frames > 1 ? cpf : 0};
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "toeplitz P1"));
+        }
     }
     const int64_t E2 = (int64_t)L2 * B;
     if (t.dim == 3) {
