@@ -19,6 +19,7 @@ from .toeplitz import (  # noqa: F401
     ToeplitzAccumulateType,
     ToeplitzMultType,
     sense_normal,
+    sense_normal_ex,
     toeplitz_kernel,
     toeplitz_multiplication,
     toeplitz_multiply,
@@ -26,6 +27,10 @@ from .toeplitz import (  # noqa: F401
 )
 from .normal import (  # noqa: F401
     BatchedNormalOp,
+    NormalIDTT1Op,
+    NormalIDTT2Op,
+    NormalIDTWT1Op,
+    NormalIDTWT2Op,
     NormalTT1Op,
     NormalTT2Op,
     SenseOffresOp,
@@ -33,7 +38,8 @@ from .normal import (  # noqa: F401
     build_toeplitz_kernel,
     build_toeplitz_kernels,
 )
-from .cg import BatchedCGSolver, CGSolver, conjugate_gradient, vdot_real  # noqa: F401
+from .cg import BatchedCGSolver, CGSolver, conjugate_gradient, conjugate_gradient_precond, vdot_real  # noqa: F401
+from .alg import max_eig  # noqa: F401
 from . import autograd  # noqa: F401
 
 __version__ = "0.1.0"

@@ -44,6 +44,7 @@ SIGNATURES = {
                                         _i, _i, _i, _i, _i, _i, _vp]),
     "hb_sense_normal": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hb_sense_normal_noalloc": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "hb_sense_normal_ex": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "hb_sense_normal_batched": (_i, [_i, _pi64, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hb_transform_toeplitz_kernels": (_i, [_i, _pi64, _i64, _vp, _vp, _vp]),
     "hb_cgb_state_bytes": (_sz, [_i64]),
@@ -54,6 +55,10 @@ SIGNATURES = {
     "hb_cg_init": (_i, [_i64, _vp, _vp, _vp, _vp, _vp, _d, _vp]),
     "hb_cg_step": (_i, [_i64, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hb_cg_read_state": (_i, [_vp, C.POINTER(_d), _pi64, C.POINTER(_i), _vp]),
+    "hb_pcg_residual": (_i, [_i64, _vp, _vp, _vp, _vp]),
+    "hb_pcg_start": (_i, [_i64, _vp, _vp, _vp, _vp, _d, _vp]),
+    "hb_pcg_step1": (_i, [_i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hb_pcg_step2": (_i, [_i64, _vp, _vp, _vp, _vp, _i, _vp]),
     "hb_vdot_real": (_i, [_i64, _vp, _vp, _vp, _vp]),
     "hb_timing_enable": (_i, [_i]),
     "hb_timing_read": (_i, [C.c_char_p, _sz, C.POINTER(_f), _i, C.POINTER(_i), C.POINTER(_i)]),

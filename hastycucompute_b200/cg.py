@@ -199,3 +199,46 @@ class BatchedCGSolver:
         cv = (C.c_int * self.nframes)()
         _lib.call("hb_cgb_read_state", ptr(self.state), self.nframes, rz, it, cv, stream_ptr(self.device))
         return list(rz), list(it), [bool(v) for v in cv]
+
+
+def conjugate_gradient_precond(A: Callable[[torch.Tensor], torch.Tensor], P: Callable[[torch.Tensor], torch.Tensor],
+                               max_inner_iter: int, max_outer_iter: int, tol: float = 1e-6):
+    """conjugate_gradient(A, P, max_inner_iter, max_outer_iter, tol) (cpp/corelib/lib/op/cg.cppm:
+    16-119): preconditioned CG with restarts. Returns ``cgl(x, b, should_restart_callback=None,
+    after_restart_callback=None) -> x`` like the reference's lambda.
+
+    The scalars stay on the device (hb_pcg_*); the reference's ``if resid < tol: break`` is the
+    device break flag, so without callbacks no iteration reads anything back. A
+    ``should_restart_callback(x) -> bool`` is a host decision per iteration, so with one the
+    driver reads the break flag first (one synchronisation per iteration), as the reference
+    evaluates ``resid`` before it. ``after_restart_callback(x)`` runs after every outer loop."""
+
+    def cgl(x: torch.Tensor, b: torch.Tensor, should_restart_callback=None, after_restart_callback=None) -> torch.Tensor:
+        check_tensor(x, "x", torch.complex64)
+        check_tensor(b, "b", torch.complex64, x.shape, x.device)
+        dev = x.device
+        n = x.numel()
+        r = torch.empty_like(x)
+        p = torch.empty_like(x)
+        state = CGState(dev)
+        _lib.call("hb_pcg_residual", n, ptr(b), ptr(A(x)), ptr(r), stream_ptr(dev))
+        z = P(r)
+        _lib.call("hb_pcg_start", n, ptr(r), ptr(z), ptr(p), ptr(state.buf), float(tol), stream_ptr(dev))
+        for _outer in range(int(max_outer_iter)):
+            for _inner in range(int(max_inner_iter)):
+                if should_restart_callback is not None and state.read(dev)[2]:
+                    break
+                Ap = A(p)
+                _lib.call("hb_pcg_step1", n, ptr(x), ptr(r), ptr(p), ptr(Ap), ptr(state.buf), stream_ptr(dev))
+                z = P(r)
+                restart = bool(should_restart_callback(x)) if should_restart_callback is not None else False
+                _lib.call("hb_pcg_step2", n, ptr(r), ptr(z), ptr(p), ptr(state.buf), 1 if restart else 0,
+                          stream_ptr(dev))
+                if restart:
+                    break
+            if after_restart_callback is not None:
+                after_restart_callback(x)
+        cgl.state = state
+        return x
+
+    return cgl

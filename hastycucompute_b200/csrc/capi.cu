@@ -25,6 +25,9 @@ int sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x, c
                  void* out, void* workspace, size_t workspace_bytes, cudaStream_t s);
 int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps,
                          const void* kernel, void* out, cudaStream_t s);
+int sense_normal_ex(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps_in,
+                    const void* smaps_out, const void* diag, int accumulate, const void* kernel, void* out,
+                    void* workspace, size_t workspace_bytes, cudaStream_t s);
 int sense_normal_batched(int dim, const int64_t* shape, int64_t nframes, int64_t ncoils, const void* x,
                          const void* smaps, const void* kernels, void* out, void* workspace, size_t workspace_bytes,
                          cudaStream_t s);
@@ -38,6 +41,10 @@ int cgb_read_state(const void* state, int64_t nf, double* rzold, int64_t* iters,
 size_t cg_state_bytes();
 int cg_init(int64_t n, const void* b, const void* Ax, void* r, void* p, void* state, double tol, cudaStream_t s);
 int cg_step(int64_t n, void* x, void* r, void* p, const void* Ap, void* state, cudaStream_t s);
+int pcg_residual(int64_t n, const void* b, const void* Ax, void* r, cudaStream_t s);
+int pcg_start(int64_t n, const void* r, const void* z, void* p, void* state, double tol, cudaStream_t s);
+int pcg_step1(int64_t n, void* x, void* r, const void* p, const void* Ap, void* state, cudaStream_t s);
+int pcg_step2(int64_t n, const void* r, const void* z, void* p, void* state, int restart, cudaStream_t s);
 int cg_read_state(const void* state, double* rzold, int64_t* iters, int* converged, cudaStream_t s);
 int vdot_real(int64_t n, const void* a, const void* b, double* out, cudaStream_t s);
 }  // namespace hb
@@ -197,6 +204,15 @@ int hb_sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const
     HB_GUARD({ return hb::sense_normal_noalloc(dim, shape, ncoils, x, smaps, kernel, out, as_stream(stream)); })
 }
 
+int hb_sense_normal_ex(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps_in,
+                       const void* smaps_out, const void* diag, int accumulate, const void* kernel, void* out,
+                       void* workspace, size_t workspace_bytes, void* stream) {
+    HB_GUARD({
+        return hb::sense_normal_ex(dim, shape, ncoils, x, smaps_in, smaps_out, diag, accumulate, kernel, out, workspace,
+                                   workspace_bytes, as_stream(stream));
+    })
+}
+
 int hb_sense_normal_batched(int dim, const int64_t* shape, int64_t nframes, int64_t ncoils, const void* x,
                             const void* smaps, const void* kernels, void* out, void* workspace, size_t workspace_bytes,
                             void* stream) {
@@ -237,6 +253,22 @@ int hb_cg_init(int64_t n, const void* b, const void* Ax, void* r, void* p, void*
 
 int hb_cg_step(int64_t n, void* x, void* r, void* p, const void* Ap, void* state, void* stream) {
     HB_GUARD({ return hb::cg_step(n, x, r, p, Ap, state, as_stream(stream)); })
+}
+
+int hb_pcg_residual(int64_t n, const void* b, const void* Ax, void* r, void* stream) {
+    HB_GUARD({ return hb::pcg_residual(n, b, Ax, r, as_stream(stream)); })
+}
+
+int hb_pcg_start(int64_t n, const void* r, const void* z, void* p, void* state, double tol, void* stream) {
+    HB_GUARD({ return hb::pcg_start(n, r, z, p, state, tol, as_stream(stream)); })
+}
+
+int hb_pcg_step1(int64_t n, void* x, void* r, const void* p, const void* Ap, void* state, void* stream) {
+    HB_GUARD({ return hb::pcg_step1(n, x, r, p, Ap, state, as_stream(stream)); })
+}
+
+int hb_pcg_step2(int64_t n, const void* r, const void* z, void* p, void* state, int restart, void* stream) {
+    HB_GUARD({ return hb::pcg_step2(n, r, z, p, state, restart, as_stream(stream)); })
 }
 
 int hb_cg_read_state(const void* state, double* rzold, int64_t* iters, int* converged, void* stream) {

@@ -176,6 +176,86 @@ __global__ void __launch_bounds__(kRedThreads) k_cg_dir(int64_t n, const float2*
     }
 }
 
+// ---- preconditioned / restarted CG (cpp/corelib/lib/op/cg.cppm:16-119) -------------------------
+//   r = b - A x; z = P r; p = z; rzold = Re<r,z>; resid = sqrt(rzold)
+//   loop: if resid < tol: break
+//         Ap = A p; alpha = rzold / Re<p,Ap>; x += alpha p; r -= alpha Ap          (step 1)
+//         z = P r                                                                   (caller)
+//         rznew = Re<r,z>; p = restart ? z : z + (rznew / rzold) p; rzold = rznew  (step 2)
+// Step 1 reuses k_cg_alpha (break test, Re<p,Ap>, alpha); the break leaves every vector as is.
+__global__ void k_pcg_residual(int64_t n, const float2* __restrict__ b, const float2* __restrict__ Ax,
+                               float2* __restrict__ r) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        r[i] = csub(b[i], Ax[i]);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_pcg_start(int64_t n, const float2* __restrict__ r,
+                                                            const float2* __restrict__ z, float2* __restrict__ p,
+                                                            CgState* st, double tol) {
+    double part = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 rv = r[i], zv = z[i];
+        p[i] = zv;
+        part += (double)rv.x * zv.x + (double)rv.y * zv.y;
+    }
+    double tot;
+    if (finish_reduction(part, st->partial, &st->counter, &tot) && threadIdx.x == 0) {
+        st->rzold = tot;
+        st->tol = tol;
+        st->iters = 0;
+        st->run = 1;
+        st->alpha = 0;
+        st->beta = 0;
+        st->pAp = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_pcg_xr(int64_t n, float2* __restrict__ x, float2* __restrict__ r,
+                                                         const float2* __restrict__ p, const float2* __restrict__ Ap,
+                                                         const CgState* st) {
+    if (!st->run) return;
+    const float alpha = (float)st->alpha;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 pv = p[i], av = Ap[i];
+        float2 xv = x[i], rv = r[i];
+        xv.x = fmaf(alpha, pv.x, xv.x);
+        xv.y = fmaf(alpha, pv.y, xv.y);
+        rv.x = fmaf(-alpha, av.x, rv.x);
+        rv.y = fmaf(-alpha, av.y, rv.y);
+        x[i] = xv;
+        r[i] = rv;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_pcg_rz(int64_t n, const float2* __restrict__ r,
+                                                         const float2* __restrict__ z, CgState* st) {
+    if (!st->run) return;
+    double part = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 rv = r[i], zv = z[i];
+        part += (double)rv.x * zv.x + (double)rv.y * zv.y;
+    }
+    double tot;
+    if (finish_reduction(part, st->partial, &st->counter, &tot) && threadIdx.x == 0) {
+        st->beta = tot / st->rzold;
+        st->rzold = tot;
+        st->iters += 1;
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_pcg_dir(int64_t n, const float2* __restrict__ z, float2* __restrict__ p,
+                                                          const CgState* st, int restart) {
+    if (!st->run) return;
+    const float beta = restart ? 0.f : (float)st->beta;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 zv = z[i];
+        float2 pv = p[i];
+        pv.x = restart ? zv.x : fmaf(beta, pv.x, zv.x);
+        pv.y = restart ? zv.y : fmaf(beta, pv.y, zv.y);
+        p[i] = pv;
+    }
+}
+
 struct DotScratch {
     unsigned int counter;
     double partial[kRedMaxBlocks];
@@ -261,6 +341,44 @@ int cg_read_state(const void* state, double* rzold, int64_t* iters, int* converg
     if (iters) *iters = h.iters;
     if (converged) *converged = (h.run == 0) || (sqrt(h.rzold) < h.tol);
     return HB_OK;
+}
+
+int pcg_residual(int64_t n, const void* b, const void* Ax, void* r, cudaStream_t s) {
+    HB_REQUIRE(n >= 1, HB_ERR_INVALID_ARG, "n must be >= 1");
+    HB_REQUIRE(b && Ax && r, HB_ERR_INVALID_ARG, "null argument");
+    k_pcg_residual<<<red_blocks(n), kRedThreads, 0, s>>>(n, (const float2*)b, (const float2*)Ax, (float2*)r);
+    return check_launch("k_pcg_residual");
+}
+
+int pcg_start(int64_t n, const void* r, const void* z, void* p, void* state, double tol, cudaStream_t s) {
+    HB_REQUIRE(n >= 1, HB_ERR_INVALID_ARG, "n must be >= 1");
+    HB_REQUIRE(r && z && p && state, HB_ERR_INVALID_ARG, "null argument");
+    HB_CUDA(cudaMemsetAsync(state, 0, sizeof(CgState), s));
+    k_pcg_start<<<red_blocks(n), kRedThreads, 0, s>>>(n, (const float2*)r, (const float2*)z, (float2*)p,
+                                                     (CgState*)state, tol);
+    return check_launch("k_pcg_start");
+}
+
+int pcg_step1(int64_t n, void* x, void* r, const void* p, const void* Ap, void* state, cudaStream_t s) {
+    HB_REQUIRE(n >= 1, HB_ERR_INVALID_ARG, "n must be >= 1");
+    HB_REQUIRE(x && r && p && Ap && state, HB_ERR_INVALID_ARG, "null argument");
+    const int g = red_blocks(n);
+    CgState* st = (CgState*)state;
+    TimedSection ts("pcg_step", s);
+    k_cg_alpha<<<g, kRedThreads, 0, s>>>(n, (const float2*)p, (const float2*)Ap, st);
+    k_pcg_xr<<<g, kRedThreads, 0, s>>>(n, (float2*)x, (float2*)r, (const float2*)p, (const float2*)Ap, st);
+    return check_launch("pcg_step1");
+}
+
+int pcg_step2(int64_t n, const void* r, const void* z, void* p, void* state, int restart, cudaStream_t s) {
+    HB_REQUIRE(n >= 1, HB_ERR_INVALID_ARG, "n must be >= 1");
+    HB_REQUIRE(r && z && p && state, HB_ERR_INVALID_ARG, "null argument");
+    const int g = red_blocks(n);
+    CgState* st = (CgState*)state;
+    TimedSection ts("pcg_step", s);
+    k_pcg_rz<<<g, kRedThreads, 0, s>>>(n, (const float2*)r, (const float2*)z, st);
+    k_pcg_dir<<<g, kRedThreads, 0, s>>>(n, (const float2*)z, (float2*)p, st, restart ? 1 : 0);
+    return check_launch("pcg_step2");
 }
 
 int vdot_real(int64_t n, const void* a, const void* b, double* out, cudaStream_t s) {

@@ -135,15 +135,20 @@ struct OpToepIn {
 };
 
 // P1 of the SENSE normal operator: column e = f * cpf + c reads S_c[idx] * x_f[idx] (cpf = 0: one
-// frame, x shared by all coils). The product is fixed at compile time.
-struct OpToepInSense : OpToepIn {
+// frame, x shared by all coils), times the diagonal m2[idx] when kDiag. The product is fixed at
+// compile time.
+template <bool kDiag>
+struct OpToepInSenseT : OpToepIn {
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
         const int64_t idx = a * N2 + l;
         const int64_t ei = cpf ? e % cpf : e;
         const int64_t m1o = cpf ? (e / cpf) * n : 0;
-        return cmul(in[ei * n + idx], m1[m1o + idx]);
+        float2 v = cmul(in[ei * n + idx], m1[m1o + idx]);
+        if constexpr (kDiag) v = cmul(v, m2[idx]);
+        return v;
     }
 };
+using OpToepInSense = OpToepInSenseT<false>;
 
 // The Toeplitz passes along the middle axis: zero-padding N -> 2N (forward) and cropping
 // 2N -> N (inverse), both at offset 0.
@@ -244,6 +249,13 @@ struct OpToepOutSense {
     int64_t N2, n;
     int64_t cpf;  // coils per frame
     int nfr;      // frames
+    const float2* odiag;  // optional: the coil sum is multiplied by conj(odiag[idx])
+    int accumulate;       // add into out instead of overwriting it
+    __device__ __forceinline__ void emit(int64_t oi, int64_t ii, float2 v) const {
+        if (odiag) v = cmulc(v, odiag[ii]);
+        if (accumulate) v = cadd(v, out[oi]);
+        out[oi] = v;
+    }
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
     __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
@@ -256,7 +268,9 @@ struct OpToepOutSense {
     __device__ __forceinline__ float2 product(int64_t a, int o, int64_t e, float2 v) const {
         return cmulc(v, smaps[(e % cpf) * n + a * N2 + o]);
     }
-    __device__ __forceinline__ void write_row(int64_t a, int o, int g, float2 v) const { out[g * n + a * N2 + o] = v; }
+    __device__ __forceinline__ void write_row(int64_t a, int o, int g, float2 v) const {
+        emit(g * n + a * N2 + o, a * N2 + o, v);
+    }
     // generic-kernel path: acc is [A_blk][nfr][Lout], zeroed on the first chunk
     __device__ __forceinline__ void store_phase(const float2* res, const PassCfg& c, int64_t a0, int64_t e0, int Ab, int Eb,
                                                 float2* acc) const {
@@ -299,7 +313,7 @@ struct OpToepOutSense {
             const int o = idx % c.Lout, rest = idx / c.Lout, gg = rest % ng, al = rest / ng;
             const int64_t a = a0 + al;
             if (a >= c.A) continue;
-            out[gg * n + a * N2 + o] = acc[idx];
+            emit(gg * n + a * N2 + o, a * N2 + o, acc[idx]);
         }
     }
 };
@@ -347,6 +361,8 @@ struct ToepArgs {
     int io_mult, in_m1, out_m1, in_m2, out_m2, accumulate;
     bool sense;
     int64_t frames = 1;  // SENSE over frames: t.B = frames * coils, kernels per frame
+    const float2* smaps_out = nullptr;  // SENSE: coil maps of the reduction (default: the input maps)
+    const float2* odiag = nullptr;      // SENSE: conj(odiag) multiplies the coil sum
 };
 
 static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream_t s) {
@@ -363,7 +379,11 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
     const int64_t cpf = a.sense ? B / a.frames : 0;  // coils per frame (SENSE)
     // P1: axis 2, pad N2 -> L2, forward
     {
-        if (a.sense) {
+        if (a.sense && a.m2) {
+            OpToepInSenseT<true> op{{a.in, a.m1, a.m2, HB_MULT_MULT, HB_MULT_MULT, W1, N2, t.n, (int64_t)L2 * B, B,
+                                     a.frames > 1 ? cpf : 0}};
+            HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "toeplitz P1"));
+        } else if (a.sense) {
             OpToepInSense op{{a.in, a.m1, nullptr, HB_MULT_MULT, HB_MULT_NONE, W1, N2, t.n, (int64_t)L2 * B, B,
                               a.frames > 1 ? cpf : 0}};
             HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "toeplitz P1"));
@@ -398,7 +418,8 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
     // P5: axis 2 inverse, crop, output ops
     {
         if (a.sense) {
-            OpToepOutSense op{W1, (int64_t)L2 * B, B, a.in, a.out, N2, t.n, cpf, (int)a.frames};
+            OpToepOutSense op{W1,   (int64_t)L2 * B,   B,       a.smaps_out ? a.smaps_out : a.in, a.out, N2, t.n, cpf,
+                              (int)a.frames, a.odiag, a.accumulate};
             HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, 0, 1,
                                    sizeof(float2) * (size_t)N2 * a.frames, s, "toeplitz P5 sense"));
         } else {
@@ -498,6 +519,32 @@ int sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x, c
     a.in_m1 = HB_MULT_MULT;
     a.in_m2 = HB_MULT_NONE;
     a.sense = true;
+    return toep_run(t, a, g.ptr, s);
+}
+
+int sense_normal_ex(int dim, const int64_t* shape, int64_t ncoils, const void* x, const void* smaps_in,
+                    const void* smaps_out, const void* diag, int accumulate, const void* kernel, void* out,
+                    void* workspace, size_t workspace_bytes, cudaStream_t s) {
+    ToepGeom t;
+    HB_TRY(toep_geom(&t, dim, shape, ncoils));
+    HB_REQUIRE(x && smaps_in && kernel && out, HB_ERR_INVALID_ARG, "x, smaps_in, kernel and out must be non-null");
+    HB_REQUIRE(out != x && out != smaps_in && out != smaps_out && out != diag, HB_ERR_INVALID_ARG,
+               "out must not alias an input");
+    HB_REQUIRE(accumulate == HB_ACC_NONE || accumulate == HB_ACC_ACCUMULATE, HB_ERR_INVALID_ARG, "Invalid accumulate_type");
+    WsGuard g;
+    HB_TRY(get_workspace(t, workspace, workspace_bytes, s, &g));
+    ToepArgs a{};
+    a.in = (const float2*)smaps_in;
+    a.out = (float2*)out;
+    a.kt = (const float2*)kernel;
+    a.m1 = (const float2*)x;
+    a.m2 = (const float2*)diag;
+    a.in_m1 = HB_MULT_MULT;
+    a.in_m2 = diag ? HB_MULT_MULT : HB_MULT_NONE;
+    a.accumulate = accumulate;
+    a.sense = true;
+    a.smaps_out = (const float2*)smaps_out;
+    a.odiag = (const float2*)diag;
     return toep_run(t, a, g.ptr, s);
 }
 
@@ -765,7 +812,7 @@ int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const vo
         HB_TRY(launch_fft_pass(op, f1, 1, E2, (int)N1, 0, (int)N1, 0, 0, 0, s, "noalloc P3"));
     }
     {
-        OpToepOutSense op{W1, E2, B, S, (float2*)out, N2, t.n, B, 1};
+        OpToepOutSense op{W1, E2, B, S, (float2*)out, N2, t.n, B, 1, nullptr, 0};
         HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, 0, 1, sizeof(float2) * (size_t)N2, s,
                                "noalloc P5 sense"));
     }

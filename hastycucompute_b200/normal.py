@@ -16,7 +16,7 @@ from typing import Optional, Sequence
 import torch
 
 from .nufft import NufftOpts, NufftPlan, NufftType
-from .toeplitz import make_workspace, sense_normal, toeplitz_kernel, transform_toeplitz_kernel
+from .toeplitz import make_workspace, sense_normal, sense_normal_ex, toeplitz_kernel, transform_toeplitz_kernel
 
 
 class NormalTT1Op:
@@ -211,3 +211,121 @@ class SenseOffresOp:
 
     def normal(self, x: torch.Tensor) -> torch.Tensor:
         return self.adjoint(self.forward(x))
+
+
+def _transform_all(kernels: torch.Tensor, transformed: bool) -> torch.Tensor:
+    if transformed:
+        return kernels.contiguous()
+    return torch.stack([transform_toeplitz_kernel(k.contiguous()) for k in kernels])
+
+
+class NormalIDTT1Op:
+    """NORMAL_IDT_T1_OP (cpp/corelib/lib/mri/normal.cppm:185-270): time-segmented SENSE normal
+    operator B x = sum_l R_l^H [sum_s Psi_s^H F^H T_l F Psi_s] R_l x, from L (kernel T_l,
+    diagonal R_l) pairs and the stacked coil maps Psi. Each segment is one fused apply (coil
+    expand, padded convolution, coil reduce, conj(R_l), accumulate into the output); the
+    reference's [C, N..] per-coil intermediate and its separate sum over coils do not exist here."""
+
+    class_name = "NORMAL_IDT_T1_OP"
+
+    def __init__(self, kernels: torch.Tensor, kerneldiags: torch.Tensor, stacked_diags: torch.Tensor,
+                 transformed: bool = False):
+        if kernels.shape[0] != kerneldiags.shape[0]:
+            raise RuntimeError("Number of kernels and kernel diagonals must match.")
+        self.kernels_t = _transform_all(kernels, transformed)
+        self.kerneldiags = kerneldiags.contiguous()
+        self.smaps = stacked_diags.contiguous()
+        self.smaps_out: Optional[torch.Tensor] = None
+        self.shape = tuple(self.smaps.shape[1:])
+        self.dim = len(self.shape)
+        if tuple(self.kerneldiags.shape[1:]) != self.shape:
+            raise ValueError("kernel diagonals must have the image shape")
+        self.workspace = make_workspace(self.shape, self.smaps.shape[0], self.smaps.device)
+
+    def apply(self, x: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty_like(x)
+        for l in range(self.kernels_t.shape[0]):
+            sense_normal_ex(x, self.smaps, self.kernels_t[l], out, self.smaps_out, self.kerneldiags[l],
+                            accumulate=l > 0, scratch=self.workspace)
+        return out
+
+    __call__ = apply
+
+
+class NormalIDTWT1Op(NormalIDTT1Op):
+    """NORMAL_IDTW_T1_OP (cpp/corelib/lib/mri/normal.cppm:405-580): B = sum_{i,j} W_ij Psi_i^H
+    [sum_l R_l^H F^H T_l F R_l] Psi_j with W the inverse noise covariance. The reference forms the
+    per-coil results, mixes them with torch.mm(W, .) and reduces with conj(Psi). Since
+    sum_i conj(Psi_i) sum_j W_ij v_j = sum_j conj(U_j) v_j with U = W^H Psi, the mixing is folded
+    once into output coil maps U and every segment stays one fused apply."""
+
+    class_name = "NORMAL_IDTW_T1_OP"
+
+    def __init__(self, kernels: torch.Tensor, kerneldiags: torch.Tensor, stacked_diags: torch.Tensor,
+                 weights: torch.Tensor, transformed: bool = False):
+        super().__init__(kernels, kerneldiags, stacked_diags, transformed)
+        C = self.smaps.shape[0]
+        if tuple(weights.shape) != (C, C):
+            raise ValueError("weights must be [C, C]")
+        self.weights = weights.contiguous()
+        self.smaps_out = torch.mm(self.weights.conj().t().contiguous(), self.smaps.reshape(C, -1)).reshape(self.smaps.shape)
+
+
+class NormalIDTT2Op:
+    """NORMAL_IDT_T2_OP (cpp/corelib/lib/mri/normal.cppm:292-372): the time-segmented operator in
+    the coil maps, (B Psi)_i = X^H [sum_l R_l^H F^H T_l F R_l] X Psi_i: for each segment one
+    batched multiplication with the reference's flags (input x and R_l, output conj(x) and
+    conj(R_l)), accumulated over segments."""
+
+    class_name = "NORMAL_IDT_T2_OP"
+
+    def __init__(self, kernels: torch.Tensor, kerneldiags: torch.Tensor, x: torch.Tensor, transformed: bool = False):
+        if kernels.shape[0] != kerneldiags.shape[0]:
+            raise RuntimeError("Number of kernels and kernel diagonals must match.")
+        self.kernels_t = _transform_all(kernels, transformed)
+        self.kerneldiags = kerneldiags.contiguous()
+        self.x = x.contiguous()
+        self.shape = tuple(self.x.shape)
+        self._ws = {}
+
+    def _segments(self, stacked_diags: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        from .toeplitz import ToeplitzAccumulateType as A, ToeplitzMultType as T, toeplitz_multiplication
+        B = stacked_diags.shape[0]
+        if B not in self._ws:
+            self._ws[B] = make_workspace(self.shape, B, self.x.device)
+        sd = stacked_diags.contiguous()
+        for l in range(self.kernels_t.shape[0]):
+            toeplitz_multiplication(sd, out, self.kernels_t[l], self._ws[B], self.x, self.kerneldiags[l], T.NONE,
+                                    T.MULT, T.MULT_CONJ, T.MULT, T.MULT_CONJ, A.ACCUMULATE if l > 0 else A.NONE)
+        return out
+
+    def apply(self, stacked_diags: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty_like(stacked_diags)
+        return self._segments(stacked_diags, out)
+
+    __call__ = apply
+
+
+class NormalIDTWT2Op(NormalIDTT2Op):
+    """NORMAL_IDTW_T2_OP (cpp/corelib/lib/mri/normal.cppm:586-720): NORMAL_IDT_T2_OP followed by
+    the coil mixing stack_out = W @ stack_out (one complex GEMM over [C, prod N])."""
+
+    class_name = "NORMAL_IDTW_T2_OP"
+
+    def __init__(self, kernels: torch.Tensor, kerneldiags: torch.Tensor, x: torch.Tensor, weights: torch.Tensor,
+                 transformed: bool = False):
+        super().__init__(kernels, kerneldiags, x, transformed)
+        self.weights = weights.contiguous()
+
+    def apply(self, stacked_diags: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        C = stacked_diags.shape[0]
+        tmp = self._segments(stacked_diags, torch.empty_like(stacked_diags))
+        mixed = torch.mm(self.weights, tmp.reshape(C, -1)).reshape(stacked_diags.shape)
+        if out is None:
+            return mixed
+        out.copy_(mixed)
+        return out
+
+    __call__ = apply

@@ -147,3 +147,26 @@ def sense_normal(x: torch.Tensor, smaps: torch.Tensor, kernel_t: torch.Tensor, o
         _lib.call("hb_sense_normal", dim, _lib.i64_array(x.shape), int(smaps.shape[0]), ptr(x), ptr(smaps),
                   ptr(kernel_t), ptr(out), ptr(scratch), sb, stream_ptr(x.device))
     return out
+
+
+def sense_normal_ex(x: torch.Tensor, smaps: torch.Tensor, kernel_t: torch.Tensor, out: torch.Tensor,
+                    smaps_out: Optional[torch.Tensor] = None, diag: Optional[torch.Tensor] = None,
+                    accumulate: bool = False, scratch: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """out (+)= conj(R) sum_c conj(U_c) T(R S_c x): one time segment of NORMAL_IDT_T1_OP /
+    NORMAL_IDTW_T1_OP (cpp/corelib/lib/mri/normal.cppm:218-266, 441-535) as one fused apply.
+    U = smaps_out (default smaps), R = diag (default 1)."""
+    dim = x.dim()
+    check_tensor(x, "x", torch.complex64)
+    check_tensor(smaps, "smaps", torch.complex64, (smaps.shape[0], *x.shape), x.device)
+    if smaps_out is not None:
+        check_tensor(smaps_out, "smaps_out", torch.complex64, tuple(smaps.shape), x.device)
+    if diag is not None:
+        check_tensor(diag, "diag", torch.complex64, tuple(x.shape), x.device)
+    check_tensor(kernel_t, "kernel", torch.complex64, tuple(2 * s for s in x.shape), x.device)
+    check_tensor(out, "out", torch.complex64, x.shape, x.device)
+    sb = 0 if scratch is None else scratch.numel() * scratch.element_size()
+    with torch.cuda.device(x.device):
+        _lib.call("hb_sense_normal_ex", dim, _lib.i64_array(x.shape), int(smaps.shape[0]), ptr(x), ptr(smaps),
+                  ptr(smaps_out), ptr(diag), 1 if accumulate else 0, ptr(kernel_t), ptr(out), ptr(scratch), sb,
+                  stream_ptr(x.device))
+    return out

@@ -170,6 +170,19 @@ int hb_sense_normal(int dim, const int64_t* shape, int64_t ncoils, const void* x
                     const void* smaps, const void* kernel, void* out,
                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* One time segment of NORMAL_IDT_T1_OP / NORMAL_IDTW_T1_OP (cpp/corelib/lib/mri/normal.cppm:
+ * 218-266 and 441-535), fused like hb_sense_normal:
+ *   out (+)= conj(R) * sum_c conj(U_c) * T(R * S_c * x)
+ * S = smaps_in [C, N..]; U = smaps_out [C, N..] (NULL: U = S); R = diag [N..] (NULL: 1).
+ * NORMAL_IDT_T1_OP is the sum of these over its L (kernel, diagonal) pairs, the first call with
+ * accumulate = HB_ACC_NONE and the rest HB_ACC_ACCUMULATE. NORMAL_IDTW_T1_OP's coil mixing
+ * sum_i conj(S_i) sum_j W_ij v_j equals sum_j conj(U_j) v_j with U_j = sum_i conj(W_ij) S_i, so it
+ * runs with U = W^H S. out must not alias an input; workspace as for hb_sense_normal. */
+int hb_sense_normal_ex(int dim, const int64_t* shape, int64_t ncoils, const void* x,
+                       const void* smaps_in, const void* smaps_out, const void* diag, int accumulate,
+                       const void* kernel, void* out, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
 /* ---- frames: many systems in one launch per pass (no counterpart in the reference) -------
  * hb_sense_normal over F frames that share the coil maps, each with its own Toeplitz kernel:
  *   out[f] = sum_c conj(S_c) T_f(S_c x[f])     x, out: [F, N..]; smaps: [C, N..]
@@ -211,6 +224,19 @@ int hb_cg_init(int64_t n, const void* b, const void* Ax, void* r, void* p, void*
 /* pAp = Re<p,Ap>; alpha = rzold/pAp; x += alpha p; r -= alpha Ap; rznew = Re<r,r>;
  * p = r + (rznew/rzold) p; rzold = rznew. */
 int hb_cg_step(int64_t n, void* x, void* r, void* p, const void* Ap, void* state, void* stream);
+/* Preconditioned / restarted CG, cpp/corelib/lib/op/cg.cppm:16-119, on the same state block:
+ *   hb_pcg_residual: r = b - Ax;   caller: z = P(r);   hb_pcg_start: p = z, rzold = Re<r,z>
+ *   iteration:  Ap = A(p); hb_pcg_step1 (break test sqrt(rzold) < tol, alpha, x, r);
+ *               z = P(r);  hb_pcg_step2 (rznew = Re<r,z>, p = z (restart != 0) or
+ *               z + (rznew/rzold) p, rzold = rznew).
+ * After the break test fires both steps leave x, r and p unchanged. */
+int hb_pcg_residual(int64_t n, const void* b, const void* Ax, void* r, void* stream);
+int hb_pcg_start(int64_t n, const void* r, const void* z, void* p, void* state, double tol,
+                 void* stream);
+int hb_pcg_step1(int64_t n, void* x, void* r, const void* p, const void* Ap, void* state,
+                 void* stream);
+int hb_pcg_step2(int64_t n, const void* r, const void* z, void* p, void* state, int restart,
+                 void* stream);
 /* Copies {rzold, iterations done, converged flag} to host (synchronises the stream). */
 int hb_cg_read_state(const void* state, double* rzold, int64_t* iters, int* converged,
                      void* stream);

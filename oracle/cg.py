@@ -45,3 +45,46 @@ def conjugate_gradient(A, b, x0, max_iter: int, tol: float = 1e-6, dtype=np.comp
         resid = np.sqrt(rzold)
         hist.append(rzold)
     return x, hist
+
+
+def conjugate_gradient_precond(A, P, b, x0, max_inner_iter: int, max_outer_iter: int, tol: float = 1e-6,
+                               should_restart=None, dtype=np.complex128):
+    """Preconditioned / restarted CG following cpp/corelib/lib/op/cg.cppm:16-119 (steps :35-56,
+    loop :66-111). ``should_restart(x, k)`` gets the iterate and the number of steps taken."""
+    x = np.array(x0, dtype=dtype)
+    b = np.asarray(b, dtype=dtype)
+    r = (b - A(x)).astype(dtype)
+    z = np.asarray(P(r), dtype=dtype)
+    p = z.copy()
+    rzold = _rdot(r, z)
+    resid = np.sqrt(rzold)
+    k = 0
+    for _outer in range(max_outer_iter):
+        for _inner in range(max_inner_iter):
+            if resid < tol:
+                break
+            Ap = np.asarray(A(p), dtype=dtype)
+            alpha = rzold / _rdot(p, Ap)
+            x = (x + alpha * p).astype(dtype)
+            r = (r - alpha * Ap).astype(dtype)
+            z = np.asarray(P(r), dtype=dtype)
+            k += 1
+            restart = bool(should_restart(x, k)) if should_restart is not None else False
+            rznew = _rdot(r, z)
+            p = z.copy() if restart else (z + (rznew / rzold) * p).astype(dtype)
+            rzold = rznew
+            resid = np.sqrt(rzold)
+            if restart:
+                break
+    return x
+
+
+def max_eig(A, x0, max_iter: int = 10):
+    """Power iteration of cpp/corelib/lib/op/alg.cppm:15-30."""
+    x = np.asarray(x0, dtype=np.complex128)
+    m = 0.0
+    for _ in range(max_iter):
+        y = np.asarray(A(x), dtype=np.complex128)
+        m = float(np.linalg.norm(y.ravel()))
+        x = y / m
+    return m, x

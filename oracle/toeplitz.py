@@ -88,3 +88,48 @@ def sense_normal(x, smaps, kernel, workers: int | None = None, dtype=np.complex1
     s = np.asarray(smaps, dtype=dtype)
     v = toeplitz_multiply(s * x[None], kernel, workers=workers, dtype=dtype)
     return np.sum(np.conj(s) * v, axis=0)
+
+
+# ---- time-segmented (and noise-weighted) normal operators, cpp/corelib/lib/mri/normal.cppm ----
+# Each restates the operator's sequence of toeplitz_multiplication calls (first without, the rest
+# with ACCUMULATE) and its TorchScript epilogue.
+
+def normal_idt_t1(kernels, kerneldiags, stacked_diags, x):
+    """NORMAL_IDT_T1_OP::operator() (normal.cppm:218-266): flags (io MULT_CONJ, in1 MULT,
+    out1 NONE, in2 MULT, out2 MULT_CONJ) with mult1 = x, mult2 = R_l, then the sum over coils."""
+    out = np.zeros(np.shape(stacked_diags), dtype=np.complex128)
+    for i in range(len(kernels)):
+        out = toeplitz_multiplication(stacked_diags, out, kernels[i], x, kerneldiags[i], MULT_CONJ, MULT, NONE, MULT,
+                                      MULT_CONJ, 1 if i > 0 else 0)
+    return out.sum(axis=0)
+
+
+def normal_idt_t2(kernels, kerneldiags, x, stacked_diags):
+    """NORMAL_IDT_T2_OP::operator() (normal.cppm:322-369): flags (io NONE, in1 MULT,
+    out1 MULT_CONJ, in2 MULT, out2 MULT_CONJ) with mult1 = x, mult2 = R_l; no coil sum."""
+    out = np.zeros(np.shape(stacked_diags), dtype=np.complex128)
+    for i in range(len(kernels)):
+        out = toeplitz_multiplication(stacked_diags, out, kernels[i], x, kerneldiags[i], NONE, MULT, MULT_CONJ, MULT,
+                                      MULT_CONJ, 1 if i > 0 else 0)
+    return out
+
+
+def normal_idtw_t1(kernels, kerneldiags, stacked_diags, weights, x):
+    """NORMAL_IDTW_T1_OP::operator() (normal.cppm:441-491) and its script (:530-534): flags (io NONE,
+    in1 MULT, out1 NONE, in2 MULT, out2 MULT_CONJ), then stack_out = W @ stack_out, times
+    conj(stacked_diags), summed over coils."""
+    out = np.zeros(np.shape(stacked_diags), dtype=np.complex128)
+    for i in range(len(kernels)):
+        out = toeplitz_multiplication(stacked_diags, out, kernels[i], x, kerneldiags[i], NONE, MULT, NONE, MULT,
+                                      MULT_CONJ, 1 if i > 0 else 0)
+    C = out.shape[0]
+    out = (np.asarray(weights, np.complex128) @ out.reshape(C, -1)).reshape(out.shape)
+    return (out * np.conj(np.asarray(stacked_diags, np.complex128))).sum(axis=0)
+
+
+def normal_idtw_t2(kernels, kerneldiags, x, weights, stacked_diags):
+    """NORMAL_IDTW_T2_OP::operator() (normal.cppm:619-668) and its script (:704-708): flags
+    (io NONE, in1 MULT, out1 MULT_CONJ, in2 MULT, out2 MULT_CONJ), then stack_out = W @ stack_out."""
+    out = normal_idt_t2(kernels, kerneldiags, x, stacked_diags)
+    C = out.shape[0]
+    return (np.asarray(weights, np.complex128) @ out.reshape(C, -1)).reshape(out.shape)
