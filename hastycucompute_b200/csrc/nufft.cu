@@ -438,9 +438,9 @@ struct SpreadSmem {
     static constexpr int kFloats = kCoefFloats + (2 * kBuf > kOut ? 2 * kBuf : kOut);
 };
 
-// Bits lo/bs .. hi/bs (inclusive) of a block mask.
-__device__ __forceinline__ unsigned block_bits(int lo, int hi, int bs) {
-    return (2u << (hi / bs)) - (1u << (lo / bs));
+// Bits lo/bs .. hi/bs (inclusive) of a block mask; bs = 1 << lbs.
+__device__ __forceinline__ unsigned block_bits(int lo, int hi, int lbs) {
+    return (2u << (hi >> lbs)) - (1u << (lo >> lbs));
 }
 
 template <int CC>
@@ -467,11 +467,13 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
     const int org0 = tz * T0, org1 = ty * T1, org2 = tx * T2;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // this thread's cell and its warp's block
-    const int nbx = T2 / wb.bx, nby = T1 / wb.by;
+    // the block edges divide the power-of-two tile edges, so they are powers of two: shifts
+    const int lbz = __ffs(wb.bz) - 1, lby = __ffs(wb.by) - 1, lbx = __ffs(wb.bx) - 1;
+    const int nbx = T2 >> lbx, nby = T1 >> lby;
     const int bxi = warp % nbx, byi = (warp / nbx) % nby, bzi = warp / (nbx * nby);
-    const int cz = bzi * wb.bz + lane / (wb.by * wb.bx);
-    const int cy = byi * wb.by + (lane / wb.bx) % wb.by;
-    const int cx = bxi * wb.bx + lane % wb.bx;
+    const int cz = (bzi << lbz) + (lane >> (lby + lbx));
+    const int cy = (byi << lby) + ((lane >> lbx) & (wb.by - 1));
+    const int cx = (bxi << lbx) + (lane & (wb.bx - 1));
     const int czb = cz + 16, cyb = cy + 16, cxb = cx + 16;
     const unsigned mz = 1u << bzi, my = 1u << (16 + byi), mx = 1u << bxi;
     const int w0 = g.wa[0], w1 = g.wa[1], w2 = g.wa[2];
@@ -552,7 +554,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                 const int ic = (int)ceilf(v);
                 const float sarg = fmaf(2.f, __fsub_rn((float)ic, v), -1.f);
                 const int nf = g.nf[ax], T = g.T[ax];
-                const int bs = ax == 0 ? wb.bz : (ax == 1 ? wb.by : wb.bx);
+                const int lbs = ax == 0 ? lbz : (ax == 1 ? lby : lbx);
                 int iw = ic;
                 if (iw < 0) iw += nf;
                 if (iw >= nf) iw -= nf;
@@ -562,12 +564,12 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                 // footprint cells rel .. rel+w-1 (mod nf) inside [0, T)
                 am = 0u;
                 if (rel < T) {
-                    am |= block_bits(rel, min(rel + w - 1, T - 1), bs);
+                    am |= block_bits(rel, min(rel + w - 1, T - 1), lbs);
                     relb = rel + 16;
                 } else {
                     relb = max(rel - nf + 16, 0);  // a footprint reaching the tile starts >= -(w-1)
                 }
-                if (rel + w - 1 >= nf) am |= block_bits(0, min(rel + w - 1 - nf, T - 1), bs);
+                if (rel + w - 1 >= nf) am |= block_bits(0, min(rel + w - 1 - nf, T - 1), lbs);
             } else {
                 wt[0] = 1.f;
             }
@@ -655,9 +657,9 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                 const int cg = cc0 + h0 + c;
                 for (int j0 = 0; j0 < 32; j0 += CPR) {
                     const int j = j0 + lane / H;
-                    const int jz = bzi * wb.bz + j / (wb.by * wb.bx);
-                    const int jy = byi * wb.by + (j / wb.bx) % wb.by;
-                    const int jx = bxi * wb.bx + j % wb.bx;
+                    const int jz = (bzi << lbz) + (j >> (lby + lbx));
+                    const int jy = (byi << lby) + ((j >> lbx) & (wb.by - 1));
+                    const int jx = (bxi << lbx) + (j & (wb.bx - 1));
                     if (cg < g.C) {
                         const int64_t gi = ((int64_t)(org0 + jz) * nf1 + (org1 + jy)) * nf2 + (org2 + jx);
                         const float2 v = ow[j * (H + 1) + c];
@@ -1433,7 +1435,8 @@ int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx) {
     const int b[3] = {bz, by, bx};
     HB_REQUIRE(bz * by * bx == 32, HB_ERR_INVALID_ARG, "warp block must hold 32 cells");
     for (int ax = 0; ax < 3; ++ax) {
-        HB_REQUIRE(b[ax] >= 1 && p->g.T[ax] % b[ax] == 0, HB_ERR_INVALID_ARG, "warp block must tile the spread tile");
+        HB_REQUIRE(b[ax] >= 1 && (b[ax] & (b[ax] - 1)) == 0 && p->g.T[ax] % b[ax] == 0, HB_ERR_INVALID_ARG,
+                   "warp block edges must be powers of two that tile the spread tile");
         HB_REQUIRE(p->g.T[ax] > 1 || b[ax] == 1, HB_ERR_INVALID_ARG, "unit axes take a block edge of 1");
     }
     p->maxp = maxp;
