@@ -717,6 +717,10 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
             }
             const int pj = a.perm[s];
             const unsigned rowstride = (unsigned)nf2 * (unsigned)g.C;
+            // Common case: the footprint wraps neither along axis 2 nor axis 1 and the lanes hold
+            // all C transforms, so a tap's column stride is the compile-time CC: one row pointer,
+            // W loads at constant offsets.
+            const bool slab_fast = (W <= 6) && g.C == CC && wy == W && i0[2] + W <= nf2 && i0[1] + W <= nf1;
             for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
                 if (cc0 + coil >= g.C) break;
                 const float2* gridc = a.grid + cc0 + coil;
@@ -725,6 +729,32 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
                     int gz = i0[0] + dz;
                     if (gz >= nf0) gz -= nf0;
                     const float wzv = wts[dz];
+                    if constexpr (W <= 6) {
+                        if (slab_fast) {
+                            const float2* p0 =
+                                gridc + (((unsigned)gz * (unsigned)nf1 + (unsigned)i0[1]) * (unsigned)nf2 + (unsigned)i0[2]) * (unsigned)CC;
+                            float2 v[W * W];
+#pragma unroll
+                            for (int dy = 0; dy < W; ++dy) {
+                                const float2* pr = p0 + (size_t)dy * rowstride;
+#pragma unroll
+                                for (int dx = 0; dx < W; ++dx) v[dy * W + dx] = pr[dx * CC];
+                            }
+#pragma unroll
+                            for (int dy = 0; dy < W; ++dy) {
+                                float rr = 0.f, ri = 0.f;
+#pragma unroll
+                                for (int dx = 0; dx < W; ++dx) {
+                                    rr = fmaf(wx[dx], v[dy * W + dx].x, rr);
+                                    ri = fmaf(wx[dx], v[dy * W + dx].y, ri);
+                                }
+                                const float wzy = wzv * wts[kMaxWidth + dy];
+                                ar = fmaf(wzy, rr, ar);
+                                ai = fmaf(wzy, ri, ai);
+                            }
+                            continue;
+                        }
+                    }
                     unsigned rowbase[W];
 #pragma unroll
                     for (int dy = 0; dy < W; ++dy) {
