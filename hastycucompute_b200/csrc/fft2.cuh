@@ -15,6 +15,7 @@
 #pragma once
 
 #include <type_traits>
+#include <utility>
 
 #include "fft.cuh"
 
@@ -41,9 +42,66 @@ __device__ __forceinline__ float2 tw_get(const float2* tw, int m) {
     return w;
 }
 
-// In-register DFT of size R; `tws` = L / R so that W_R^m = tw[m * tws].
+// ---- compile-time twiddles -----------------------------------------------------------------
+// W_R^m = exp(-2 pi i m / R) evaluated while compiling: the angle is reduced to [-pi, pi] and
+// sine / cosine are summed from their Taylor series in double (terms to x^31, error far below
+// float rounding), then rounded once to float. Exact quarter turns become swaps.
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+constexpr double ct_sin(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 16; ++k) {
+        term *= -x * x / (double)((2 * k) * (2 * k + 1));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double ct_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 16; ++k) {
+        term *= -x * x / (double)((2 * k - 1) * (2 * k));
+        sum += term;
+    }
+    return sum;
+}
+template <int R, int M>
+constexpr double ct_angle() {
+    constexpr int m = ((M % R) + R) % R;
+    return kTwoPi * (double)(2 * m > R ? m - R : m) / (double)R;  // in [-pi, pi]
+}
+
+// a * W_R^M (INV: conjugate twiddle)
+template <int R, int M, bool INV>
+__device__ __forceinline__ float2 cmul_tw(float2 a) {
+    constexpr int m = ((M % R) + R) % R;
+    if constexpr (m == 0) {
+        return a;
+    } else if constexpr (4 * m == R) {
+        return INV ? mul_pi(a) : mul_mi(a);  // -i (forward) / +i (inverse)
+    } else if constexpr (2 * m == R) {
+        return make_float2(-a.x, -a.y);
+    } else if constexpr (4 * m == 3 * R) {
+        return INV ? mul_mi(a) : mul_pi(a);
+    } else {
+        constexpr float c = (float)ct_cos(ct_angle<R, M>());
+        constexpr float sn = (float)(INV ? ct_sin(ct_angle<R, M>()) : -ct_sin(ct_angle<R, M>()));
+        return make_float2(fmaf(a.x, c, -a.y * sn), fmaf(a.x, sn, a.y * c));
+    }
+}
+
+// Calls f(std::integral_constant<int, I>) for I = 0 .. N-1 (indices usable as constants).
+template <class F, int... I>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+    static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
+// In-register DFT of size R (composite sizes split as A x B with constant twiddles).
 template <int R, bool INV>
-__device__ __forceinline__ void dft_reg(float2* v, const float2* tw, int tws) {
+__device__ __forceinline__ void dft_reg(float2* v, const float2* = nullptr, int = 0) {
     if constexpr (R == 1) {
         return;
     } else if constexpr (IsBaseRadix<R>::value) {
@@ -52,21 +110,23 @@ __device__ __forceinline__ void dft_reg(float2* v, const float2* tw, int tws) {
         constexpr int A = split_factor<R>();
         constexpr int B = R / A;
         float2 y[R];
-#pragma unroll
-        for (int t = 0; t < B; ++t) {
+        static_for<B>([&](auto tc) {
+            constexpr int t = decltype(tc)::value;
             float2 a[A];
 #pragma unroll
             for (int j = 0; j < A; ++j) a[j] = v[t + B * j];
             dft<A, INV>(a);
-#pragma unroll
-            for (int k1 = 0; k1 < A; ++k1) y[t * A + k1] = (t * k1 == 0) ? a[k1] : cmul(a[k1], tw_get<INV>(tw, t * k1 * tws));
-        }
+            static_for<A>([&](auto kc) {
+                constexpr int k1 = decltype(kc)::value;
+                y[t * A + k1] = cmul_tw<R, t * k1, INV>(a[k1]);
+            });
+        });
 #pragma unroll
         for (int k1 = 0; k1 < A; ++k1) {
             float2 b[B];
 #pragma unroll
             for (int t = 0; t < B; ++t) b[t] = y[t * A + k1];
-            dft_reg<B, INV>(b, tw, tws * A);
+            dft_reg<B, INV>(b);
 #pragma unroll
             for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = b[k2];
         }
@@ -76,19 +136,19 @@ __device__ __forceinline__ void dft_reg(float2* v, const float2* tw, int tws) {
 // DFT of size R whose inputs v[R/2..R) are zero: X[2m] = DFT_{R/2}(v)[m],
 // X[2m+1] = DFT_{R/2}(v_j W_R^j)[m].
 template <int R, bool INV>
-__device__ __forceinline__ void dft_reg_halfzero(float2* v, const float2* tw, int tws) {
+__device__ __forceinline__ void dft_reg_halfzero(float2* v, const float2* = nullptr, int = 0) {
     if constexpr (R % 2 != 0 || R < 4) {
-        dft_reg<R, INV>(v, tw, tws);
+        dft_reg<R, INV>(v);
     } else {
         constexpr int H = R / 2;
         float2 a[H], b[H];
-#pragma unroll
-        for (int j = 0; j < H; ++j) {
+        static_for<H>([&](auto jc) {
+            constexpr int j = decltype(jc)::value;
             a[j] = v[j];
-            b[j] = j == 0 ? v[0] : cmul(v[j], tw_get<INV>(tw, j * tws));
-        }
-        dft_reg<H, INV>(a, tw, tws * 2);
-        dft_reg<H, INV>(b, tw, tws * 2);
+            b[j] = cmul_tw<R, j, INV>(v[j]);
+        });
+        dft_reg<H, INV>(a);
+        dft_reg<H, INV>(b);
 #pragma unroll
         for (int m = 0; m < H; ++m) {
             v[2 * m] = a[m];
