@@ -40,6 +40,7 @@ from .normal import (  # noqa: F401
 )
 from .cg import BatchedCGSolver, CGSolver, conjugate_gradient, conjugate_gradient_precond, vdot_real  # noqa: F401
 from .alg import max_eig  # noqa: F401
+from .pipeline import HostPipeline  # noqa: F401
 from . import autograd  # noqa: F401
 
 __version__ = "0.1.0"
