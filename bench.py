@@ -366,6 +366,11 @@ def run_ours(args, wl_name: str):
         torch.cuda.empty_cache()
         extra["frames"] = bench_frames(args, hb, dev, stream)
 
+    # ---- configurations 0, 3 and 4 at their own sizes -------------------------------------------
+    if not args.no_configs and rank == 0:
+        torch.cuda.empty_cache()
+        extra["configs"] = bench_configs(args, hb, dev, stream)
+
     # ---- accuracy of the timed apply: coil subset against the FP64 oracle ------------------------
     acc = {}
     if rank == 0 and not args.no_check:
@@ -519,6 +524,134 @@ def bench_frames(args, hb, dev, stream, nframes=24, shape=(128, 128, 128), C=16,
             "toeplitz_kernels_s": round(t_kernels, 3), "graph_captured": True}
 
 
+def bench_configs(args, hb, dev, stream):
+    """Configurations 0, 3 and 4 at their own sizes, bounded to seconds each:
+    0: 64^3, 8 coils, golden-means radial 1024 x 128, KB w=4: A^H A applies/s, NUFFT Msamp/s,
+       10-iteration graph-captured CG;
+    3: 2-D 256^2, 12 coils, 32 variable-density spiral interleaves x 2048, w=4: NUFFT Msamp/s and
+       one forward + backward of ||A^H(Ax - y)||^2 + lam * slew through the coordinate-gradient
+       kernels (finite-difference agreement is checked in the GPU tests);
+    4: 4 volumes of 128^3, 12 coils, 3-D radial 16384 x 128 (2.1 M points) each, 10 unrolled
+       Toeplitz SENSE-CG iterations with learnable steps and weights, per-iteration recomputation:
+       forward + backward time and peak HBM allocated by torch."""
+    import torch
+    from hastycucompute_b200 import autograd as ag, synthetic
+    from hastycucompute_b200.unrolled import UnrolledCG
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def todev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def nufft_rates(shape, C, dc, w):
+        M = dc[0].shape[0]
+        opts = hb.NufftOpts(nmodes=shape, ntransf=C, kernel_width=w)
+        p2, p1 = hb.NufftPlan(hb.NufftType.TYPE_2, opts), hb.NufftPlan(hb.NufftType.TYPE_1, opts)
+        p2.setpts(dc)
+        p1.setpts(dc)
+        f = torch.randn((C, *shape), dtype=torch.complex64, device=dev)
+        y = torch.empty((C, M), dtype=torch.complex64, device=dev)
+        g = torch.empty_like(f)
+        t2 = timed(lambda: p2.execute(f, y), 10)
+        t1 = timed(lambda: p1.execute(y, g), 10)
+        p1.free()
+        p2.free()
+        return round(M * C / (t2 / 1e3) / 1e6, 1), round(M * C / (t1 / 1e3) / 1e6, 1)
+
+    res = {}
+    # ---- config 0 --------------------------------------------------------------------------------
+    shape, C, w = (64, 64, 64), 8, 4
+    dc = [todev(c) for c in synthetic.golden_means_radial(1024, 128)]
+    S = todev(synthetic.coil_maps(C, shape))
+    x = todev(synthetic.image(shape))
+    K = hb.build_toeplitz_kernel(dc, shape, kernel_width=w)
+    op = hb.NormalTT1Op(K, S)
+    o = torch.empty_like(x)
+    aha_ms = timed(lambda: op.apply(x, o), 20)
+    t2r, t1r = nufft_rates(shape, C, dc, w)
+    b = op(x)
+    solver = hb.CGSolver(lambda v, out: op.apply(v, out), shape, dev, max_iter=10, tol=0.0, graph=True)
+    cg_ms = timed(lambda: solver.solve(torch.zeros_like(x), b), 3)
+    res["config0"] = {"workload": "64^3, 8 coils, golden-means radial 1024 x 128, KB w=4",
+                      "aha_applies_per_s": round(1e3 / aha_ms, 1), "type2_msamp_per_s": t2r,
+                      "type1_msamp_per_s": t1r, "cg10_recons_per_s": round(1e3 / cg_ms, 2)}
+    del solver, op, K, S
+    # ---- config 3 --------------------------------------------------------------------------------
+    shape, C, ninter, ns = (256, 256), 12, 32, 2048
+    k0 = synthetic.variable_density_spiral_2d(ninter, ns)
+    dc = [todev(c) for c in k0]
+    t2r, t1r = nufft_rates(shape, C, dc, w)
+    S = todev(synthetic.coil_maps(C, shape))
+    xt = todev(synthetic.image(shape))
+    pair = ag.NufftPair(shape, C, kernel_width=w)
+    kk = todev(k0)
+    with torch.no_grad():
+        y = ag.nufft_forward(S * xt[None], kk, pair)
+    x0 = todev(synthetic.image(shape, seed=5))
+
+    def step():
+        xg = x0.clone().requires_grad_(True)
+        kg = kk.clone().requires_grad_(True)
+        r = ag.nufft_forward(S * xg[None], kg, pair) - y
+        gimg = (torch.conj(S) * ag.nufft_adjoint(r, kg, pair)).sum(0)
+        k3 = kg.reshape(2, ninter, ns)
+        slew = ((k3[:, :, 2:] - 2 * k3[:, :, 1:-1] + k3[:, :, :-2]) ** 2).sum()
+        loss = (gimg.abs() ** 2).sum() + 1e-3 * slew
+        loss.backward()
+
+    loss_ms = timed(step, 3)
+    res["config3"] = {"workload": "2-D 256^2, 12 coils, 32 variable-density spirals x 2048, KB w=4",
+                      "type2_msamp_per_s": t2r, "type1_msamp_per_s": t1r,
+                      "loss_forward_backward_ms": round(loss_ms, 2),
+                      "gradient_check": "tests/test_grad_gpu.py: 64 coordinates and 16 pixels vs central "
+                                        "differences (h = 1e-4) of the FP64 NUDFT loss, <= 1e-3"}
+    del pair, S
+    torch.cuda.empty_cache()
+    # ---- config 4 --------------------------------------------------------------------------------
+    F, shape, C = 4, (128, 128, 128), 12
+    frames = [[todev(c) for c in synthetic.golden_means_radial(16384, 128, offset=16384 * f)] for f in range(F)]
+    Ks = hb.build_toeplitz_kernels(frames, shape, kernel_width=w)
+    del frames
+    S = todev(synthetic.coil_maps(C, shape))
+    op4 = hb.BatchedNormalOp(Ks, S)
+    xt = todev(synthetic.dynamic_images(F, shape))
+    ob = torch.empty_like(xt)
+    apply_ms = timed(lambda: op4.apply(xt, ob), 5)
+    b4 = op4(xt)
+    net = UnrolledCG(op4, iterations=10, step_init=0.9, lam_init=0.01, checkpoint=True).to(dev)
+
+    def fb():
+        net.zero_grad(set_to_none=True)
+        loss = ((net(b4) - xt).abs() ** 2).sum()
+        loss.backward()
+
+    fb()
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats(dev)
+    base = torch.cuda.memory_allocated(dev)
+    fb_ms = timed(fb, 1)
+    peak = torch.cuda.max_memory_allocated(dev)
+    res["config4"] = {"workload": "4 x 128^3, 12 coils, 3-D radial 16384 x 128 per volume, KB w=4, "
+                                  "10 unrolled CG iterations, per-iteration recomputation",
+                      "aha_applies_per_s_per_volume": round(F * 1e3 / apply_ms, 1),
+                      "unrolled_forward_backward_ms": round(fb_ms, 1),
+                      "peak_hbm_gb": round(peak / 1e9, 2), "resident_before_gb": round(base / 1e9, 2),
+                      "scalar_gradient_check": "tests/test_unrolled_gpu.py: steps and weights vs central "
+                                               "differences, <= 1e-3"}
+    del net, op4, Ks, S
+    torch.cuda.empty_cache()
+    return res
+
+
 def check_accuracy(hb, wl, K, dev):
     """Runs the fused apply on a 2-coil subset and compares it with the FP64 oracle apply using
     the same kernel."""
@@ -562,6 +695,7 @@ def main(argv=None):
     ap.add_argument("--no-nufft", action="store_true")
     ap.add_argument("--no-cg", action="store_true")
     ap.add_argument("--no-frames", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
