@@ -480,21 +480,54 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
     const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
 
     for (int i = tid; i < kCoefFloats; i += kSpreadThreads) coef[i] = (&a.kb.coef[0][0])[i];
-    if (tid == 0) {
-        int n = 0, acc = 0;
-        for_each_nbr_bin(g.nb, tz, ty, tx, [&](int bin) {
-            const int st = a.bin_start[bin];
-            s_start[n] = st;
-            s_pref[n] = acc;
-            acc += a.bin_start[bin + 1] - st;
-            ++n;
-        });
-        s_pref[n] = acc;
-        s_nbin = n;
+    // the (up to 8) bins whose points reach the tile, in for_each_nbr_bin order: one lane each,
+    // offsets by a shuffle scan
+    if (warp == 0) {
+        const int nz = g.nb[0] > 1 ? 2 : 1, ny = g.nb[1] > 1 ? 2 : 1, nx = g.nb[2] > 1 ? 2 : 1;
+        const int nbn = nz * ny * nx;
+        int st = 0, cnt = 0;
+        if (lane < nbn) {
+            const int dx = lane % nx, dy = (lane / nx) % ny, dz = lane / (nx * ny);
+            const int bz = (tz - dz + g.nb[0]) % g.nb[0], by = (ty - dy + g.nb[1]) % g.nb[1];
+            const int bx = (tx - dx + g.nb[2]) % g.nb[2];
+            const int bin = (bz * g.nb[1] + by) * g.nb[2] + bx;
+            st = a.bin_start[bin];
+            cnt = a.bin_start[bin + 1] - st;
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < nbn) {
+            s_start[lane] = st;
+            s_pref[lane] = incl - cnt;
+        }
+        if (lane == nbn - 1) {
+            s_pref[nbn] = incl;
+            s_nbin = nbn;
+        }
     }
     __syncthreads();
     const int nbin = s_nbin;
     const int total = s_pref[nbin];
+    if (total == 0) {
+        // no point reaches the tile: zero its cells with 16-byte stores (rows of T2 cells x C
+        // transforms are contiguous and 16-byte aligned: T2 and the tile origin are multiples of 8)
+        if (!extra_mode) {
+            const int rowf4 = (T2 * g.C) >> 1;
+            const int nrow = T0 * T1;
+            for (int i = tid; i < nrow * rowf4; i += kSpreadThreads) {
+                const int r = i / rowf4, c4 = i - r * rowf4;
+                const int zz = r / T1, yy = r - zz * T1;
+                float4* dst = reinterpret_cast<float4*>(
+                    a.grid + (((int64_t)(org0 + zz) * nf1 + (org1 + yy)) * nf2 + org2) * g.C);
+                dst[c4] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        return;
+    }
     const int k_begin = chunk * a.maxp;
     const int k_end = min(total, k_begin + a.maxp);
     const float hw = a.kb.hw;
@@ -1108,6 +1141,20 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
     return HB_OK;
 }
 
+// Candidates per spread subproblem when the caller has not set one: every point is a candidate
+// of up to 2^d tiles; aim at about 32 subproblems per SM so that the dense tiles of centre-heavy
+// trajectories (radial, spirals) split across the GPU, with at least 256 and at most 4096
+// candidates (large problems keep long chunks per CTA).
+static int auto_subproblem(int64_t M, const GridGeom& g) {
+    int64_t cand = M;
+    for (int ax = 0; ax < 3; ++ax)
+        if (g.nb[ax] > 1) cand *= 2;
+    const int64_t want = cand / ((int64_t)kNumSMs * 32);
+    int m = 256;
+    while (m < want && m < 4096) m <<= 1;
+    return m;
+}
+
 int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const float* c2, cudaStream_t s) {
     GridGeom& g = p->g;
     HB_REQUIRE(M >= 0 && M < (int64_t)0x7fffffff, HB_ERR_INVALID_ARG, "M must be in [0, 2^31)");
@@ -1198,6 +1245,7 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
         for (int ax = 0; ax < 3; ++ax)
             if (!ca[ax] && p->su[ax] && M > 0) cudaMemsetAsync(p->su[ax], 0, sizeof(float) * M, s);
         if (p->type == 1) {
+            if (p->maxp_auto) p->maxp = auto_subproblem(M, g);
             TileNbr tn;
             for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
             k_tile_extra_count<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins,
@@ -1470,6 +1518,7 @@ int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx) {
         HB_REQUIRE(p->g.T[ax] > 1 || b[ax] == 1, HB_ERR_INVALID_ARG, "unit axes take a block edge of 1");
     }
     p->maxp = maxp;
+    p->maxp_auto = false;
     for (int ax = 0; ax < 3; ++ax) p->wb[ax] = b[ax];
     return HB_OK;
 }

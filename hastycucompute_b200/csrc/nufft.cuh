@@ -54,8 +54,10 @@ struct NufftPlan {
     int64_t extra_cap = 0;
     int* d_err = nullptr;
     bool pts_set = false;
-    // spreading knobs (autotuned): candidates per subproblem and the warp's cell block
+    // spreading knobs (autotuned): candidates per subproblem and the warp's cell block. Unless set
+    // explicitly, the subproblem size is chosen at setpts from the number of points.
     int maxp = 4096;
+    bool maxp_auto = true;
     int wb[3] = {2, 4, 4};
     size_t device_bytes = 0;
 };

@@ -153,7 +153,8 @@ class NufftPlan:
     # -- extras ----------------------------------------------------------------------------------
     def set_spread_tuning(self, max_candidates: int = 4096, block=(2, 4, 4)) -> None:
         """Spreading knobs (before setpts): points per subproblem and the warp's cell block
-        (image order; 2-D plans take (1, by, bx))."""
+        (image order; 2-D plans take (1, by, bx)). Without a call, setpts picks the subproblem
+        size from the number of points."""
         if self.M is not None:
             raise RuntimeError("set the spread tuning before setpts")
         b = tuple(int(v) for v in block)

@@ -98,8 +98,9 @@ int hb_nufft_setpts(hb_nufft_plan plan, int64_t M, const float* coord0, const fl
 int hb_nufft_execute(hb_nufft_plan plan, const void* in, void* out, void* stream);
 
 /* Spreading knobs (no counterpart in the reference; set by the autotuner, before setpts): points
- * per spread subproblem (32..65536, default 4096) and the cell block a warp owns inside a spread
- * tile (32 cells; default 2x4x4 in 3-D, 1x4x8 in 2-D; each edge divides the tile edge, unit axes 1). */
+ * per spread subproblem (32..65536; when never set, setpts picks a power of two in 512..4096 from
+ * the number of points) and the cell block a warp owns inside a spread tile (32 cells; default
+ * 2x4x4 in 3-D, 1x4x8 in 2-D; power-of-two edges dividing the tile edge, unit axes 1). */
 int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block_z, int block_y,
                                int block_x);
 
