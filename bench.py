@@ -226,8 +226,8 @@ def workload_config(wl):
 # our arm
 
 # DRAM traffic / algorithmic bytes of the fused pass P3 from one ncu capture at 160^3 x 8 coils
-# (profiles/pass2_OpToepMid_prof160.md: 1.310833 GB read + 1.228160 GB written for 2.359296 GB
-# algorithmic); traffic and algorithmic bytes both grow with (coils + 1), so the ratio carries over.
+# (1.310833 GB read + 1.228160 GB written for 2.359296 GB algorithmic); traffic and algorithmic
+# bytes both grow with (coils + 1), so the ratio carries over.
 P3_TRAFFIC_RATIO = (1.310833e9 + 1.228160e9) / 2.359296e9
 
 
