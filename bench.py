@@ -147,7 +147,7 @@ def dist_setup(use_gpu: bool):
 
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl" if use_gpu else "gloo", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl" if use_gpu else "gloo", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
