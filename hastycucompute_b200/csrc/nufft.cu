@@ -650,11 +650,11 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                         if (dz < 0) dz += nf0;
                         if (dy < 0) dy += nf1;
                         if (dx < 0) dx += nf2;
-                        float wgt = 0.f;
-                        if (dz < w0 && dy < w1 && dx < w2) {
-                            const float* wq = bwt + q * 3 * kMaxWidth;
-                            wgt = wq[dz] * wq[kMaxWidth + dy] * wq[2 * kMaxWidth + dx];
-                        }
+                        // branch-free: outside the footprint read tap 0 and select weight 0
+                        const bool in = dz < w0 && dy < w1 && dx < w2;
+                        const float* wq = bwt + q * 3 * kMaxWidth;
+                        const float wp = wq[in ? dz : 0] * wq[kMaxWidth + (in ? dy : 0)] * wq[2 * kMaxWidth + (in ? dx : 0)];
+                        const float wgt = in ? wp : 0.f;
                         const float2* vq = bval + q * CC;
                         if constexpr (CC == 1) {
                             const float2 v = vq[0];
