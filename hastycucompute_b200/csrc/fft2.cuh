@@ -173,6 +173,17 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Op::kStageRow (optional, default false): on zero-padded inputs each sample is
+// load_col(a, l, e) * row(a)[l] (or * row_at(a, l, e) when !row_shared()).
+template <class Op, class = void>
+struct StageRow {
+    static constexpr bool value = false;
+};
+template <class Op>
+struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
+    static constexpr bool value = Op::kStageRow;
+};
+
 // Op contract (in addition to fft.cuh's):
 //   static constexpr bool kStoreLFast    // destination contiguous along the output index
 //   static constexpr bool kSenseReduce   // sum over inner columns into one output row
@@ -208,6 +219,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
     float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][groups][Lout] running sums
     float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * op.ngroups() * c.Lout : 0);  // kFusedK: [kMaxKCols][L]
     float2* Ss = Ks + (Op::kFusedK ? kMaxKCols * L : 0);          // kSenseReduce: [W][Lout]
+    float2* Rs = Ss + (Op::kSenseReduce ? c.W * c.Lout : 0);      // StageRow: [A_blk][L/2]
 
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
         tw[i] = c.tw[i];
@@ -281,7 +293,37 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             const bool colok = col < c.W && a < c.A && e < c.E;
             float2 v[P];
             bool halfzero;
-            if constexpr (kHalfIn) {
+            if constexpr (kHalfIn && StageRow<Op>::value) {
+                // sample = column factor (own load) x row factor shared by the CTA's columns of
+                // the same row: the rows go through shared memory once instead of one global load
+                // per column
+                constexpr int H = L / 2;
+                const bool staged = op.row_shared();
+                if (staged) {
+                    for (int i = tid; i < c.A_blk * H; i += blockDim.x) {
+                        const int ar = i / H, lr = i - ar * H;
+                        if (a0 + ar < c.A) cp_async8(Rs + i, op.row(a0 + ar) + lr);
+                    }
+                    cp_async_commit();
+                }
+#pragma unroll
+                for (int j = 0; j < P; ++j)
+                    v[j] = (j < P / 2 && colok) ? op.load_col(a, t + Q * j, e) : make_float2(0.f, 0.f);
+                if (staged) {
+                    cp_async_wait_all();
+                    __syncthreads();
+                    // only real columns: a padding column's al can be A_blk, past the staged rows
+                    if (colok) {
+#pragma unroll
+                        for (int j = 0; j < P / 2; ++j) v[j] = cmul(v[j], Rs[al * H + t + Q * j]);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < P / 2; ++j)
+                        if (colok) v[j] = cmul(v[j], op.row_at(a, t + Q * j, e));
+                }
+                halfzero = true;
+            } else if constexpr (kHalfIn) {
 #pragma unroll
                 for (int j = 0; j < P; ++j)
                     v[j] = (j < P / 2 && colok) ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
@@ -523,6 +565,7 @@ int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s,
     size_t smem = (size_t)((Op::kFusedK || !Op::kLoadLFast ? 2 : 1) * L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
     if (Op::kFusedK) smem += (size_t)kMaxKCols * L * sizeof(float2);
     if (Op::kSenseReduce) smem += (size_t)c.W * c.Lout * sizeof(float2);
+    if (StageRow<Op>::value) smem += (size_t)c.A_blk * (L / 2) * sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op, HM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // the staging passes want every CTA they can fit; plain passes keep the default L1 split
     if (e == cudaSuccess && (Op::kFusedK || Op::kSenseReduce))

@@ -140,10 +140,19 @@ struct OpToepIn {
 template <bool kDiag>
 struct OpToepInSenseT : OpToepIn {
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
+        return cmul(load_col(a, l, e), row_at(a, l, e));
+    }
+    // the image factor x is the same for every coil column of a row (one frame): the pass stages
+    // it once per CTA
+    static constexpr bool kStageRow = true;
+    __device__ __forceinline__ bool row_shared() const { return cpf == 0; }
+    __device__ __forceinline__ const float2* row(int64_t a) const { return m1 + a * N2; }
+    __device__ __forceinline__ float2 row_at(int64_t a, int l, int64_t e) const {
+        return m1[(cpf ? (e / cpf) * n : 0) + a * N2 + l];
+    }
+    __device__ __forceinline__ float2 load_col(int64_t a, int l, int64_t e) const {
         const int64_t idx = a * N2 + l;
-        const int64_t ei = cpf ? e % cpf : e;
-        const int64_t m1o = cpf ? (e / cpf) * n : 0;
-        float2 v = cmul(in[ei * n + idx], m1[m1o + idx]);
+        float2 v = in[(cpf ? e % cpf : e) * n + idx];
         if constexpr (kDiag) v = cmul(v, m2[idx]);
         return v;
     }
