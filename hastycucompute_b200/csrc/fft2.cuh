@@ -174,7 +174,8 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // Op::kStageRow (optional, default false): on zero-padded inputs each sample is
-// load_col(a, l, e) * row(a)[l] (or * row_at(a, l, e) when !row_shared()).
+// load_col(a, l, e) * row(a, e0)[l] when row_shared(e0, E_blk) (one row factor for all columns
+// e0 .. e0+E_blk-1 of a row), else load_col(a, l, e) * row_at(a, l, e).
 template <class Op, class = void>
 struct StageRow {
     static constexpr bool value = false;
@@ -298,11 +299,11 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
                 // the same row: the rows go through shared memory once instead of one global load
                 // per column
                 constexpr int H = L / 2;
-                const bool staged = op.row_shared();
+                const bool staged = op.row_shared(e0, c.E_blk);
                 if (staged) {
                     for (int i = tid; i < c.A_blk * H; i += blockDim.x) {
                         const int ar = i / H, lr = i - ar * H;
-                        if (a0 + ar < c.A) cp_async8(Rs + i, op.row(a0 + ar) + lr);
+                        if (a0 + ar < c.A) cp_async8(Rs + i, op.row(a0 + ar, e0) + lr);
                     }
                     cp_async_commit();
                 }

@@ -177,15 +177,15 @@ __global__ void k_scan_add(int* out, const int* sums, int64_t n) {
     if (i < n) out[i] += sums[blockIdx.x];
 }
 
-int exclusive_scan_int(const int* in, int* out, int64_t n, cudaStream_t s) {
+int exclusive_scan_int(const int* in, int* out, int64_t n, cudaStream_t s, int* sums) {
     const int64_t nb = ceil_div(std::max<int64_t>(n, 1), kScanBlock);
-    int* sums = nullptr;
-    HB_CUDA(cudaMallocAsync(&sums, sizeof(int) * nb, s));
+    const bool own = sums == nullptr;
+    if (own) HB_CUDA(cudaMallocAsync(&sums, sizeof(int) * nb, s));
     k_scan_blocks<<<(unsigned)nb, kScanBlock, 0, s>>>(in, out, sums, n);
     k_scan_sums<<<1, kScanBlock, 0, s>>>(sums, nb, out + n);
     k_scan_add<<<(unsigned)nb, kScanBlock, 0, s>>>(out, sums, n);
     int st = check_launch("exclusive_scan_int");
-    HB_CUDA(cudaFreeAsync(sums, s));
+    if (own) HB_CUDA(cudaFreeAsync(sums, s));
     return st;
 }
 
@@ -1182,33 +1182,34 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
     g.M = M;
     p->pts_set = false;
 
-    // temporaries
-    float* u[3] = {nullptr, nullptr, nullptr};
-    int *binid = nullptr, *rank = nullptr, *count = nullptr, *ecnt = nullptr, *eoff = nullptr;
-    auto cleanup = [&]() {
-        for (int ax = 0; ax < 3; ++ax)
-            if (u[ax]) cudaFree(u[ax]);
-        if (binid) cudaFree(binid);
-        if (rank) cudaFree(rank);
-        if (count) cudaFree(count);
-        if (ecnt) cudaFree(ecnt);
-        if (eoff) cudaFree(eoff);
-    };
+    // scratch held by the plan (allocated on the first setpts, per-point arrays grown with M)
     int st = HB_OK;
+    if (p->tmp_count == nullptr) {
+        const int64_t nb = ceil_div(std::max<int64_t>(p->nbins, 1), kScanBlock);
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_count, sizeof(int) * (p->nbins + 1), "bin counts"));
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_ecnt, sizeof(int) * (p->nbins + 1), "subproblem counts"));
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_eoff, sizeof(int) * (p->nbins + 1), "subproblem offsets"));
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_sums, sizeof(int) * nb, "scan sums"));
+    }
+    if (M > p->tmp_cap) {
+        for (int ax = 0; ax < 3; ++ax) {
+            if (p->tmp_u[ax]) cudaFree(p->tmp_u[ax]);
+            p->tmp_u[ax] = nullptr;
+        }
+        if (p->tmp_binid) cudaFree(p->tmp_binid);
+        if (p->tmp_rank) cudaFree(p->tmp_rank);
+        p->tmp_binid = p->tmp_rank = nullptr;
+        p->tmp_cap = 0;
+        for (int ax = 0; ax < 3; ++ax)
+            if (ca[ax]) HB_TRY(dev_alloc(p, (void**)&p->tmp_u[ax], sizeof(float) * M, "fine coordinates"));
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_binid, sizeof(int) * M, "bin ids"));
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_rank, sizeof(int) * M, "bin ranks"));
+        p->tmp_cap = M;
+    }
+    float* u[3] = {ca[0] ? p->tmp_u[0] : nullptr, ca[1] ? p->tmp_u[1] : nullptr, ca[2] ? p->tmp_u[2] : nullptr};
+    int *binid = p->tmp_binid, *rank = p->tmp_rank, *count = p->tmp_count, *ecnt = p->tmp_ecnt, *eoff = p->tmp_eoff;
     do {
         cudaError_t e = cudaSuccess;
-        for (int ax = 0; ax < 3 && e == cudaSuccess; ++ax)
-            if (ca[ax]) e = cudaMalloc(&u[ax], sizeof(float) * std::max<int64_t>(M, 1));
-        if (e == cudaSuccess) e = cudaMalloc(&binid, sizeof(int) * std::max<int64_t>(M, 1));
-        if (e == cudaSuccess) e = cudaMalloc(&rank, sizeof(int) * std::max<int64_t>(M, 1));
-        if (e == cudaSuccess) e = cudaMalloc(&count, sizeof(int) * (p->nbins + 1));
-        if (e == cudaSuccess) e = cudaMalloc(&ecnt, sizeof(int) * (p->nbins + 1));
-        if (e == cudaSuccess) e = cudaMalloc(&eoff, sizeof(int) * (p->nbins + 1));
-        if (e != cudaSuccess) {
-            set_error(std::string("setpts temporaries: ") + cudaGetErrorString(e));
-            st = HB_ERR_ALLOC;
-            break;
-        }
         if ((e = cudaMemsetAsync(count, 0, sizeof(int) * (p->nbins + 1), s)) != cudaSuccess ||
             (e = cudaMemsetAsync(p->d_err, 0, sizeof(int), s)) != cudaSuccess) {
             set_error(std::string("setpts memset: ") + cudaGetErrorString(e));
@@ -1234,7 +1235,7 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             k_fold_bin<<<(unsigned)ceil_div(M, 256), 256, 0, s>>>(fa);
             if ((st = check_launch("k_fold_bin")) != HB_OK) break;
         }
-        if ((st = exclusive_scan_int(count, p->bin_start, p->nbins, s)) != HB_OK) break;
+        if ((st = exclusive_scan_int(count, p->bin_start, p->nbins, s, p->tmp_sums)) != HB_OK) break;
         if (M > 0) {
             k_scatter_sorted<<<(unsigned)ceil_div(M, 256), 256, 0, s>>>(u[0], u[1], u[2], binid, rank, p->bin_start,
                                                                        ca[0] ? p->su[0] : nullptr, ca[1] ? p->su[1] : nullptr,
@@ -1251,7 +1252,7 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             k_tile_extra_count<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins,
                                                                                 p->maxp, ecnt);
             if ((st = check_launch("k_tile_extra_count")) != HB_OK) break;
-            if ((st = exclusive_scan_int(ecnt, eoff, p->nbins, s)) != HB_OK) break;
+            if ((st = exclusive_scan_int(ecnt, eoff, p->nbins, s, p->tmp_sums)) != HB_OK) break;
             int n_extra = 0, err = 0;
             if ((e = cudaMemcpyAsync(&n_extra, eoff + p->nbins, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
@@ -1292,7 +1293,6 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             }
         }
     } while (0);
-    cleanup();
     if (st == HB_OK) p->pts_set = true;
     return st;
 }
@@ -1558,6 +1558,15 @@ void plan_free(NufftPlan* p) {
     if (p->bin_start) cudaFree(p->bin_start);
     if (p->extra) cudaFree(p->extra);
     if (p->d_err) cudaFree(p->d_err);
+    for (int ax = 0; ax < 3; ++ax) {
+        if (p->tmp_u[ax]) cudaFree(p->tmp_u[ax]);
+        p->tmp_u[ax] = nullptr;
+    }
+    for (int** q : {&p->tmp_binid, &p->tmp_rank, &p->tmp_count, &p->tmp_ecnt, &p->tmp_eoff, &p->tmp_sums}) {
+        if (*q) cudaFree(*q);
+        *q = nullptr;
+    }
+    p->tmp_cap = 0;
     p->X = p->Y = nullptr;
     p->perm = nullptr;
     p->inT = nullptr;

@@ -54,6 +54,16 @@ struct NufftPlan {
     int64_t extra_cap = 0;
     int* d_err = nullptr;
     bool pts_set = false;
+    // setpts scratch, kept by the plan so that re-pointing it allocates nothing: per point
+    // (grown with M) and per bin (allocated at the first setpts)
+    float* tmp_u[3] = {nullptr, nullptr, nullptr};
+    int* tmp_binid = nullptr;
+    int* tmp_rank = nullptr;
+    int64_t tmp_cap = 0;
+    int* tmp_count = nullptr;
+    int* tmp_ecnt = nullptr;
+    int* tmp_eoff = nullptr;
+    int* tmp_sums = nullptr;  // scan block sums
     // spreading knobs (autotuned): candidates per subproblem and the warp's cell block. Unless set
     // explicitly, the subproblem size is chosen at setpts from the number of points.
     int maxp = 4096;
@@ -74,6 +84,7 @@ int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx);
 void plan_free(NufftPlan* p);
 
 // Pieces reused by the Toeplitz kernel builder.
-int exclusive_scan_int(const int* in, int* out, int64_t n, cudaStream_t s);
+// `sums` (optional): ceil(n / 1024) ints of scratch; without it the scan allocates stream-ordered.
+int exclusive_scan_int(const int* in, int* out, int64_t n, cudaStream_t s, int* sums = nullptr);
 
 }  // namespace hb

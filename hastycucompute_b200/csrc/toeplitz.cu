@@ -142,11 +142,15 @@ struct OpToepInSenseT : OpToepIn {
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
         return cmul(load_col(a, l, e), row_at(a, l, e));
     }
-    // the image factor x is the same for every coil column of a row (one frame): the pass stages
-    // it once per CTA
+    // the image factor x is the same for every coil column of a row within one frame: when a
+    // CTA's columns e0 .. e0+eb-1 lie in one frame the pass stages that row once per CTA
     static constexpr bool kStageRow = true;
-    __device__ __forceinline__ bool row_shared() const { return cpf == 0; }
-    __device__ __forceinline__ const float2* row(int64_t a) const { return m1 + a * N2; }
+    __device__ __forceinline__ bool row_shared(int64_t e0, int eb) const {
+        return cpf == 0 || e0 / cpf == (e0 + eb - 1) / cpf;
+    }
+    __device__ __forceinline__ const float2* row(int64_t a, int64_t e0) const {
+        return m1 + (cpf ? (e0 / cpf) * n : 0) + a * N2;
+    }
     __device__ __forceinline__ float2 row_at(int64_t a, int l, int64_t e) const {
         return m1[(cpf ? (e / cpf) * n : 0) + a * N2 + l];
     }
