@@ -242,6 +242,17 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
         eb_end = eb_begin + 1;
     }
     const int64_t a0 = ab * c.A_blk;
+    // column -> (row in the block, inner index); with one row per CTA (every large problem) the
+    // runtime division by E_blk is skipped
+    auto split_col = [&](int col, int& al, int& el) {
+        if (c.A_blk == 1) {
+            al = 0;
+            el = col;
+        } else {
+            al = col / c.E_blk;
+            el = col - al * c.E_blk;
+        }
+    };
     if constexpr (Op::kSenseReduce) {
         for (int i = tid; i < c.A_blk * op.ngroups() * c.Lout; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
         __syncthreads();
@@ -252,10 +263,11 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
         // ---- stage the kernel columns / factor rows this chunk needs (asynchronous) -----------
         int64_t kc0 = 0;
         bool k_staged = false;
+        int nk = 1;
         if constexpr (Op::kFusedK) {
             const int64_t elast = min(e0 + c.E_blk, c.E) - 1;
             kc0 = op.kcol(e0);
-            const int nk = (int)(op.kcol(elast) - kc0 + 1);
+            nk = (int)(op.kcol(elast) - kc0 + 1);
             k_staged = (c.A_blk == 1) && nk <= kMaxKCols;
             if (k_staged) {
                 for (int i = tid; i < nk * L; i += blockDim.x) cp_async8(Ks + i, op.kptr(kc0 + i / L) + (i % L));
@@ -289,7 +301,8 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
                 col = tid % kCW;
                 t = tid / kCW;
             }
-            const int al = col / c.E_blk, el = col % c.E_blk;
+            int al, el;
+            split_col(col, al, el);
             const int64_t a = a0 + al, e = e0 + el;
             const bool colok = col < c.W && a < c.A && e < c.E;
             float2 v[P];
@@ -373,7 +386,8 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             col2 = tid % kCW;
             k1 = tid / kCW;
         }
-        const int al2 = col2 / c.E_blk, el2 = col2 % c.E_blk;
+        int al2, el2;
+        split_col(col2, al2, el2);
         const int64_t a2 = a0 + al2, e2 = e0 + el2;
         const bool colok2 = s2active && col2 < c.W && a2 < c.A && e2 < c.E;
         float2 u[Q];
@@ -392,7 +406,8 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             __syncthreads();
             if (s2active) {
                 if (k_staged) {
-                    const float2* kc = Ks + (int)(op.kcol(e2) - kc0) * L;
+                    // one kernel column for the whole block (the common case) needs no division
+                    const float2* kc = Ks + (nk == 1 ? 0 : (int)(op.kcol(e2) - kc0)) * L;
 #pragma unroll
                     for (int k2 = 0; k2 < Q; ++k2) u[k2] = colok2 ? cmul(u[k2], kc[k1 + P * k2]) : make_float2(0.f, 0.f);
                 } else {
@@ -416,7 +431,8 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduc
             // thread (col, n2): inverse P-point DFT over k1 -> x[n2 + Q n1]
             {
                 const int col3 = tid % kCW, n2 = tid / kCW;
-                const int al3 = col3 / c.E_blk, el3 = col3 % c.E_blk;
+                int al3, el3;
+                split_col(col3, al3, el3);
                 const int64_t a3 = a0 + al3, e3 = e0 + el3;
                 const bool colok3 = col3 < c.W && a3 < c.A && e3 < c.E;
                 float2 z[P];
