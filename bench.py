@@ -226,9 +226,9 @@ def workload_config(wl):
 # our arm
 
 # DRAM traffic / algorithmic bytes of the fused pass P3 from one ncu capture at 160^3 x 8 coils
-# (1.310833 GB read + 1.228160 GB written for 2.359296 GB algorithmic); traffic and algorithmic
+# (1.311066 GB read + 1.097650 GB written for 2.359296 GB algorithmic); traffic and algorithmic
 # bytes both grow with (coils + 1), so the ratio carries over.
-P3_TRAFFIC_RATIO = (1.310833e9 + 1.228160e9) / 2.359296e9
+P3_TRAFFIC_RATIO = (1.311066e9 + 1.097650e9) / 2.359296e9
 
 
 def aha_bytes(n: int, C: int, dim: int = 3) -> dict:
