@@ -72,8 +72,6 @@ struct NufftPlan {
     size_t device_bytes = 0;
 };
 
-// Candidates (points of the up to 8 bins that can reach a tile) per spread subproblem.
-constexpr int kSpreadMaxCand = 1024;
 
 int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, int ntransf, float tol,
               int width, double upsampfac, int method);
