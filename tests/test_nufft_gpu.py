@@ -187,6 +187,36 @@ def test_plan_reuse_and_resetpts(cuda):
 
 
 @pytest.mark.gpu
+def test_type1_resetpts_reuses_scratch(cuda):
+    """Type-1 plans keep their sort scratch between setpts calls: re-pointing with more, fewer and
+    again more points (different densities) gives fresh, correct results each time."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(14)
+    nm = (14, 12, 16)
+    p = _plan(hb, hb.NufftType.TYPE_1, nm, 3, 5)
+    for M, spread in ((2000, np.pi), (9000, 0.3), (400, np.pi), (12000, 1.0)):
+        coords = [rng.uniform(-spread, spread, M).astype(np.float32) for _ in range(3)]
+        c = crand(rng, 3, M)
+        p.setpts([to_dev(x, cuda) for x in coords])
+        assert relerr(to_np(p(to_dev(c, cuda))), gridding.nufft1(coords, c, nm, w=5)) <= PARITY
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nmodes", [(48, 40, 44), (96, 80)])
+def test_type1_mostly_empty_grid(cuda, nmodes):
+    """A few points in a large grid: almost every spread tile has no candidate and is zeroed by the
+    empty-tile path; the result matches the oracle everywhere."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(15)
+    M = 60
+    coords = rand_coords(rng, len(nmodes), M)
+    c = crand(rng, 2, M)
+    p = _plan(hb, hb.NufftType.TYPE_1, nmodes, 2, 4)
+    p.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p(to_dev(c, cuda))), gridding.nufft1(coords, c, nmodes, w=4)) <= PARITY
+
+
+@pytest.mark.gpu
 def test_plan_info_matches_oracle_grid(cuda):
     import hastycucompute_b200 as hb
     for nm, w in [((64, 64, 64), 4), ((160, 160, 160), 6), ((256, 256), 4), ((319, 319, 319), 6)]:
