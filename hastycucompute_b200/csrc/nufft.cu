@@ -231,14 +231,24 @@ __global__ void k_tile_extra_fill(const int* extra_cnt, const int* extra_off, in
 // ---------------------------------------------------------------------------------------------
 // execute kernels
 
-// inT[s][c] = in[c][perm[s]]  (sorted, transforms interleaved)
-__global__ void k_permute_in(const float2* __restrict__ in, const int* __restrict__ perm, float2* __restrict__ inT,
-                             int64_t M, int C) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= M * C) return;
-    const int c = (int)(idx % C);
-    const int64_t s = idx / C;
-    inT[idx] = in[(int64_t)c * M + perm[s]];
+// xin[j][c] = in[c][j]: the caller's [C][M] values with the transforms interleaved, in the
+// caller's point order (a tiled transpose, coalesced on both sides). Spreading reads the values of
+// sorted point s as the contiguous row xin[perm[s]].
+__global__ void k_interleave_in(const float2* __restrict__ in, float2* __restrict__ xin, int64_t M, int C) {
+    __shared__ float2 tile[32][33];
+    const int64_t j0 = (int64_t)blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int c = c0 + r;
+        const int64_t j = j0 + threadIdx.x;
+        if (c < C && j < M) tile[r][threadIdx.x] = in[(int64_t)c * M + j];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int64_t j = j0 + r;
+        const int c = c0 + threadIdx.x;
+        if (c < C && j < M) xin[j * C + c] = tile[threadIdx.x][r];
+    }
 }
 
 struct GridArgs {
@@ -246,7 +256,7 @@ struct GridArgs {
     const float* su[3];
     const int* perm;
     const int* bin_start;
-    const float2* inT;  // spread input [M][C]
+    const float2* inT;  // spread input [M][C], transforms interleaved, caller's point order
     float2* grid;       // [nf0][nf1][nf2][C]
     float2* out;        // interp output [C][M]
     const int2* extra;
@@ -359,7 +369,7 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
             point_setup(a, coef, s, valid, coil, CC, wts, i0);
             __syncwarp();
             if (valid && coil_ok) {
-                const float2 v = a.inT[s * g.C + cc0 + coil];
+                const float2 v = a.inT[(int64_t)a.perm[s] * g.C + cc0 + coil];
                 int r0 = i0[0] - o0, r1 = i0[1] - o1, r2 = i0[2] - o2;
                 if (r0 < 0) r0 += g.nf[0];
                 if (r1 < 0) r1 += g.nf[1];
@@ -557,7 +567,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
         // the CC values of each point (asynchronous)
         if constexpr (CC == 1) {
             for (int q = tid; q < n; q += kSpreadThreads) {
-                if (cc0 < g.C) cp_async8(bval + q, a.inT + (int64_t)sorted_index(base + q) * g.C + cc0);
+                if (cc0 < g.C) cp_async8(bval + q, a.inT + (int64_t)a.perm[sorted_index(base + q)] * g.C + cc0);
             }
         } else {
             constexpr int CP = CC / 2;
@@ -565,7 +575,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                 const int q = i / CP, c = 2 * (i % CP);
                 float2* dst = bval + q * CC + c;
                 const int cg = cc0 + c;
-                const float2* src = a.inT + (int64_t)sorted_index(base + q) * g.C + cg;
+                const float2* src = a.inT + (int64_t)a.perm[sorted_index(base + q)] * g.C + cg;
                 if (vec && cg < g.C) {
                     cp_async16(dst, src);
                 } else {
@@ -1176,7 +1186,7 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
         for (int ax = 0; ax < 3; ++ax)
             if (ca[ax] || g.nf[ax] > 1) HB_TRY(dev_alloc(p, (void**)&p->su[ax], sizeof(float) * M, "sorted coords"));
         HB_TRY(dev_alloc(p, (void**)&p->perm, sizeof(int) * M, "perm"));
-        if (p->type == 1) HB_TRY(dev_alloc(p, (void**)&p->inT, sizeof(float2) * M * g.C, "sorted input"));
+        if (p->type == 1) HB_TRY(dev_alloc(p, (void**)&p->inT, sizeof(float2) * M * g.C, "interleaved input"));
         p->M_cap = M;
     }
     g.M = M;
@@ -1437,9 +1447,10 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
 
     if (p->type == 1) {
         if (M > 0) {
-            TimedSection ts("permute_in", s);
-            k_permute_in<<<(unsigned)ceil_div(M * C, 256), 256, 0, s>>>(in, p->perm, p->inT, M, C);
-            HB_TRY(check_launch("k_permute_in"));
+            TimedSection ts("interleave_in", s);
+            k_interleave_in<<<dim3((unsigned)ceil_div(M, 32), (unsigned)ceil_div(C, 32)), dim3(32, 8), 0, s>>>(
+                in, p->inT, M, C);
+            HB_TRY(check_launch("k_interleave_in"));
         }
         GridArgs a = grid_args(p);
         HB_TRY(dispatch_cc(spread_cc(g), p, a, s, true));

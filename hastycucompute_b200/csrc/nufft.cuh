@@ -46,7 +46,7 @@ struct NufftPlan {
     int64_t M_cap = 0;
     float* su[3] = {nullptr, nullptr, nullptr};
     int* perm = nullptr;
-    float2* inT = nullptr;  // type 1: [M][C] sorted copy of the input
+    float2* inT = nullptr;  // type 1: [M][C] input with the transforms interleaved (caller point order)
     int* bin_start = nullptr;
     int64_t nbins = 0;
     int2* extra = nullptr;  // spread subproblems beyond the first chunk of each tile
