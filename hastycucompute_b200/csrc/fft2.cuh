@@ -200,8 +200,17 @@ struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
 // (Lin == L/2, in_shift == 0), so only samples j < P/2 of step 1 are loaded and the P-point DFT
 // skips the zero half; bit 1 = the output is the first half (Lout == L/2, out_shift == 0), so
 // step 2 stores k2 < Q/2 (fused passes: step 3 stores n1 < P/2) with no position checks.
+//
+// CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (95 registers; at 64 it spills
+// and runs slower), the fused-kernel and staged-row passes 3 (64 registers; at 2 CTAs they run
+// slower), the plain strided passes 4 (48 registers, a few spilled words): they move bytes, and
+// the fourth CTA hides more of the load latency than the spills cost.
+template <class Op>
+constexpr int pass2_min_blocks() {
+    return Op::kSenseReduce ? 2 : (Op::kFusedK || StageRow<Op>::value) ? 3 : 4;
+}
 template <int P, int Q, class Op, int HM = 0>
-__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : (Op::kSenseReduce ? 2 : 3)) pass2_kernel(const Op op, const PassCfg c) {
+__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks<Op>()) pass2_kernel(const Op op, const PassCfg c) {
     constexpr int L = P * Q;
     constexpr int CWp = kCW + 1;
     constexpr bool kHalfIn = (HM & 1) != 0;
