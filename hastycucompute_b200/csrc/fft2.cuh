@@ -199,7 +199,9 @@ struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
 // HM (compile-time pass shape): bit 0 = the input is zero-padded to twice its length at offset 0
 // (Lin == L/2, in_shift == 0), so only samples j < P/2 of step 1 are loaded and the P-point DFT
 // skips the zero half; bit 1 = the output is the first half (Lout == L/2, out_shift == 0), so
-// step 2 stores k2 < Q/2 (fused passes: step 3 stores n1 < P/2) with no position checks.
+// step 2 stores k2 < Q/2 (fused passes: step 3 stores n1 < P/2) with no position checks. A
+// non-zero HM also fixes the side its bits leave out at the full length L with shift 0, so those
+// loads and stores go to compile-time positions as well.
 //
 // CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (95 registers; at 64 it spills
 // and runs slower), the fused-kernel and staged-row passes 3 (64 registers; at 2 CTAs they run
@@ -215,6 +217,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
     constexpr int CWp = kCW + 1;
     constexpr bool kHalfIn = (HM & 1) != 0;
     constexpr bool kHalfOut = (HM & 2) != 0;
+    constexpr bool kExact = HM != 0;  // the side that is not halved is all L positions, unshifted
     static_assert(!kHalfIn || P % 2 == 0, "half input needs an even P");
     static_assert(!kHalfOut || (P % 2 == 0 && Q % 2 == 0), "half output needs even P and Q");
     extern __shared__ float2 smem2[];
@@ -351,6 +354,10 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 for (int j = 0; j < P; ++j)
                     v[j] = (j < P / 2 && colok) ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
                 halfzero = true;
+            } else if constexpr (kExact) {
+#pragma unroll
+                for (int j = 0; j < P; ++j) v[j] = colok ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
+                halfzero = false;
             } else {
 #pragma unroll
                 for (int j = 0; j < P; ++j) {
@@ -455,6 +462,9 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                     if constexpr (kHalfOut) {
 #pragma unroll
                         for (int n1 = 0; n1 < P / 2; ++n1) op.store(a3, n2 + Q * n1, e3, z[n1]);
+                    } else if constexpr (kExact) {
+#pragma unroll
+                        for (int n1 = 0; n1 < P; ++n1) op.store(a3, n2 + Q * n1, e3, z[n1]);
                     } else {
 #pragma unroll
                         for (int n1 = 0; n1 < P; ++n1) {
@@ -473,6 +483,9 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 if constexpr (kHalfOut) {
 #pragma unroll
                     for (int k2 = 0; k2 < Q / 2; ++k2) Y[(k1 + P * k2) * CWp + col2] = u[k2];
+                } else if constexpr (kExact) {
+#pragma unroll
+                    for (int k2 = 0; k2 < Q; ++k2) Y[(k1 + P * k2) * CWp + col2] = u[k2];
                 } else {
 #pragma unroll
                     for (int k2 = 0; k2 < Q; ++k2) {
@@ -527,6 +540,9 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 if constexpr (kHalfOut) {
 #pragma unroll
                     for (int k2 = 0; k2 < Q / 2; ++k2) op.store(a2, k1 + P * k2, e2, u[k2]);
+                } else if constexpr (kExact) {
+#pragma unroll
+                    for (int k2 = 0; k2 < Q; ++k2) op.store(a2, k1 + P * k2, e2, u[k2]);
                 } else {
 #pragma unroll
                     for (int k2 = 0; k2 < Q; ++k2) {
@@ -581,8 +597,8 @@ int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s,
     constexpr int HM = HalfIO<Op>::value;
     if constexpr (HM != 0) {
         const int in_sh = ((c.in_shift % L) + L) % L, out_sh = ((c.out_shift % L) + L) % L;
-        const bool ok_in = !(HM & 1) || (2 * c.Lin == L && in_sh == 0);
-        const bool ok_out = !(HM & 2) || (2 * c.Lout == L && out_sh == 0);
+        const bool ok_in = in_sh == 0 && ((HM & 1) ? 2 * c.Lin == L : c.Lin == L);
+        const bool ok_out = out_sh == 0 && ((HM & 2) ? 2 * c.Lout == L : c.Lout == L);
         if (!ok_in || !ok_out) {
             set_error(std::string(name) + ": pass shape does not match the operator's padding / crop");
             return HB_ERR_INVALID_ARG;
