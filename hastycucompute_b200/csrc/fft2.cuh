@@ -204,12 +204,12 @@ struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
 // loads and stores go to compile-time positions as well.
 //
 // CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (95 registers; at 64 it spills
-// and runs slower), the fused-kernel and staged-row passes 3 (64 registers; at 2 CTAs they run
-// slower), the plain strided passes 4 (48 registers, a few spilled words): they move bytes, and
-// the fourth CTA hides more of the load latency than the spills cost.
+// and runs slower), the fused-kernel pass 3 (64 registers; at 2 CTAs it runs slower), every other
+// pass 4 (48 registers, a few spilled words): they move bytes, and the fourth CTA hides more of
+// the load latency than the spills cost.
 template <class Op>
 constexpr int pass2_min_blocks() {
-    return Op::kSenseReduce ? 2 : (Op::kFusedK || StageRow<Op>::value) ? 3 : 4;
+    return Op::kSenseReduce ? 2 : Op::kFusedK ? 3 : 4;
 }
 template <int P, int Q, class Op, int HM = 0>
 __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks<Op>()) pass2_kernel(const Op op, const PassCfg c) {
