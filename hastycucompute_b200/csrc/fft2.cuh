@@ -200,8 +200,10 @@ struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
 // (Lin == L/2, in_shift == 0), so only samples j < P/2 of step 1 are loaded and the P-point DFT
 // skips the zero half; bit 1 = the output is the first half (Lout == L/2, out_shift == 0), so
 // step 2 stores k2 < Q/2 (fused passes: step 3 stores n1 < P/2) with no position checks. A
-// non-zero HM also fixes the side its bits leave out at the full length L with shift 0, so those
-// loads and stores go to compile-time positions as well.
+// halved operator also fixes the side its bits leave out at the full length L with shift 0, so
+// those loads and stores go to compile-time positions as well. Bits 2 / 3 declare the same for
+// the input / output of an operator without a fixed shape (kHalfIO 0): the launcher picks them
+// from the pass's lengths and shifts.
 //
 // CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (95 registers; at 64 it spills
 // and runs slower), the fused-kernel pass 3 (64 registers; at 2 CTAs it runs slower), every other
@@ -217,7 +219,10 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
     constexpr int CWp = kCW + 1;
     constexpr bool kHalfIn = (HM & 1) != 0;
     constexpr bool kHalfOut = (HM & 2) != 0;
-    constexpr bool kExact = HM != 0;  // the side that is not halved is all L positions, unshifted
+    // all L positions, unshifted: the side a halved operator leaves out, or bits 2 / 3
+    constexpr bool kFullIn = !kHalfIn && ((HM & 2) != 0 || (HM & 4) != 0);
+    constexpr bool kFullOut = !kHalfOut && ((HM & 1) != 0 || (HM & 8) != 0);
+    static_assert(!((HM & 1) && (HM & 4)) && !((HM & 2) && (HM & 8)), "a side is either half or full");
     static_assert(!kHalfIn || P % 2 == 0, "half input needs an even P");
     static_assert(!kHalfOut || (P % 2 == 0 && Q % 2 == 0), "half output needs even P and Q");
     extern __shared__ float2 smem2[];
@@ -354,7 +359,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 for (int j = 0; j < P; ++j)
                     v[j] = (j < P / 2 && colok) ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
                 halfzero = true;
-            } else if constexpr (kExact) {
+            } else if constexpr (kFullIn) {
 #pragma unroll
                 for (int j = 0; j < P; ++j) v[j] = colok ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
                 halfzero = false;
@@ -462,7 +467,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                     if constexpr (kHalfOut) {
 #pragma unroll
                         for (int n1 = 0; n1 < P / 2; ++n1) op.store(a3, n2 + Q * n1, e3, z[n1]);
-                    } else if constexpr (kExact) {
+                    } else if constexpr (kFullOut) {
 #pragma unroll
                         for (int n1 = 0; n1 < P; ++n1) op.store(a3, n2 + Q * n1, e3, z[n1]);
                     } else {
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 if constexpr (kHalfOut) {
 #pragma unroll
                     for (int k2 = 0; k2 < Q / 2; ++k2) Y[(k1 + P * k2) * CWp + col2] = u[k2];
-                } else if constexpr (kExact) {
+                } else if constexpr (kFullOut) {
 #pragma unroll
                     for (int k2 = 0; k2 < Q; ++k2) Y[(k1 + P * k2) * CWp + col2] = u[k2];
                 } else {
@@ -540,7 +545,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 if constexpr (kHalfOut) {
 #pragma unroll
                     for (int k2 = 0; k2 < Q / 2; ++k2) op.store(a2, k1 + P * k2, e2, u[k2]);
-                } else if constexpr (kExact) {
+                } else if constexpr (kFullOut) {
 #pragma unroll
                     for (int k2 = 0; k2 < Q; ++k2) op.store(a2, k1 + P * k2, e2, u[k2]);
                 } else {
@@ -591,23 +596,8 @@ struct HalfIO<Op, std::void_t<decltype(Op::kHalfIO)>> {
     static constexpr int value = Op::kHalfIO;
 };
 
-template <int P, int Q, class Op>
-int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s, const char* name) {
-    constexpr int L = P * Q;
-    constexpr int HM = HalfIO<Op>::value;
-    if constexpr (HM != 0) {
-        const int in_sh = ((c.in_shift % L) + L) % L, out_sh = ((c.out_shift % L) + L) % L;
-        const bool ok_in = in_sh == 0 && ((HM & 1) ? 2 * c.Lin == L : c.Lin == L);
-        const bool ok_out = out_sh == 0 && ((HM & 2) ? 2 * c.Lout == L : c.Lout == L);
-        if (!ok_in || !ok_out) {
-            set_error(std::string(name) + ": pass shape does not match the operator's padding / crop");
-            return HB_ERR_INVALID_ARG;
-        }
-    }
-    size_t smem = (size_t)((Op::kFusedK || !Op::kLoadLFast ? 2 : 1) * L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
-    if (Op::kFusedK) smem += (size_t)kMaxKCols * L * sizeof(float2);
-    if (Op::kSenseReduce) smem += (size_t)c.W * c.Lout * sizeof(float2);
-    if (StageRow<Op>::value) smem += (size_t)c.A_blk * (L / 2) * sizeof(float2);
+template <int P, int Q, class Op, int HM>
+int launch_pass2_inst(const Op& op, const PassCfg& c, size_t smem, int64_t blocks, cudaStream_t s, const char* name) {
     cudaError_t e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op, HM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // the staging passes want every CTA they can fit; plain passes keep the default L1 split
     if (e == cudaSuccess && (Op::kFusedK || Op::kSenseReduce))
@@ -617,6 +607,29 @@ int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s,
         set_error(std::string(name) + ": cudaFuncSetAttribute failed: " + cudaGetErrorString(e));
         return HB_ERR_CUDA;
     }
+    TimedSection ts(name, s);
+    pass2_kernel<P, Q, Op, HM><<<(unsigned)blocks, Q * kCW, smem, s>>>(op, c);
+    return check_launch(name);
+}
+
+template <int P, int Q, class Op>
+int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s, const char* name) {
+    constexpr int L = P * Q;
+    constexpr int HM = HalfIO<Op>::value;
+    const int in_sh = ((c.in_shift % L) + L) % L, out_sh = ((c.out_shift % L) + L) % L;
+    const bool full_in = c.Lin == L && in_sh == 0, full_out = c.Lout == L && out_sh == 0;
+    if constexpr (HM != 0) {
+        const bool ok_in = (HM & 1) ? (2 * c.Lin == L && in_sh == 0) : full_in;
+        const bool ok_out = (HM & 2) ? (2 * c.Lout == L && out_sh == 0) : full_out;
+        if (!ok_in || !ok_out) {
+            set_error(std::string(name) + ": pass shape does not match the operator's padding / crop");
+            return HB_ERR_INVALID_ARG;
+        }
+    }
+    size_t smem = (size_t)((Op::kFusedK || !Op::kLoadLFast ? 2 : 1) * L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
+    if (Op::kFusedK) smem += (size_t)kMaxKCols * L * sizeof(float2);
+    if (Op::kSenseReduce) smem += (size_t)c.W * c.Lout * sizeof(float2);
+    if (StageRow<Op>::value) smem += (size_t)c.A_blk * (L / 2) * sizeof(float2);
     const int64_t n_ab = ceil_div(c.A, c.A_blk);
     const int64_t blocks = Op::kChunkLoop ? n_ab : n_ab * c.n_eb;
     if (blocks <= 0) return HB_OK;
@@ -624,9 +637,15 @@ int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s,
         set_error(std::string(name) + ": grid too large");
         return HB_ERR_INVALID_ARG;
     }
-    TimedSection ts(name, s);
-    pass2_kernel<P, Q, Op, HM><<<(unsigned)blocks, Q * kCW, smem, s>>>(op, c);
-    return check_launch(name);
+    if constexpr (HM != 0) {
+        return launch_pass2_inst<P, Q, Op, HM>(op, c, smem, blocks, s, name);
+    } else {
+        // no fixed shape: a side that spans all L positions unshifted gets compile-time positions
+        if (full_in && full_out) return launch_pass2_inst<P, Q, Op, 12>(op, c, smem, blocks, s, name);
+        if (full_in) return launch_pass2_inst<P, Q, Op, 4>(op, c, smem, blocks, s, name);
+        if (full_out) return launch_pass2_inst<P, Q, Op, 8>(op, c, smem, blocks, s, name);
+        return launch_pass2_inst<P, Q, Op, 0>(op, c, smem, blocks, s, name);
+    }
 }
 
 // Runs the register kernel when L has one, otherwise the generic shared-memory kernel.
