@@ -25,6 +25,55 @@ def test_library_exports_header_symbols():
     assert set(names) == set(_lib.SIGNATURES), "binding table and header disagree"
 
 
+_SCALARS = {"int": C.c_int, "int64_t": C.c_int64, "float": C.c_float, "double": C.c_double,
+             "size_t": C.c_size_t, "hb_nufft_plan": C.c_void_p}
+_POINTEES = {"int": C.c_int, "int64_t": C.c_int64, "float": C.c_float, "double": C.c_double,
+             "size_t": C.c_size_t, "hb_nufft_plan": C.c_void_p}
+
+
+def declarations():
+    """{name: (return type, [parameter types])} from the header, const and names stripped."""
+    text = (ROOT / "include" / "hasty_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for ret, name, params in re.findall(r"([A-Za-z_][\w \*]*?)\s*\b(hb_\w+)\s*\(([^)]*)\)\s*;", text):
+        types = []
+        for p in params.split(","):
+            p = " ".join(p.replace("const", " ").split())
+            if p in ("", "void"):
+                continue
+            types.append(re.sub(r"\s*\b\w+$", "", p).replace(" ", "") if not p.endswith("*") else p.replace(" ", ""))
+        out[name] = (" ".join(ret.replace("const", " ").split()).replace(" *", "*"), types)
+    return out
+
+
+def _matches(ctype, ctext):
+    """ctypes type against a C type: scalars exactly; pointers as c_void_p / c_char_p or a
+    POINTER to the same pointee."""
+    if ctext.endswith("*"):
+        base = ctext[:-1]
+        if ctype in (C.c_void_p,):
+            return True
+        if ctype is C.c_char_p:
+            return base == "char"
+        return getattr(ctype, "_type_", None) is _POINTEES.get(base)
+    return ctype is _SCALARS.get(ctext)
+
+
+def test_binding_signatures_match_header():
+    """Every ctypes signature has the header's arity, pointer-ness and scalar types (a drifted
+    argument list would pass garbage through the ABI without any error)."""
+    from hastycucompute_b200 import _lib
+    decl = declarations()
+    assert set(decl) == set(_lib.SIGNATURES)
+    for name, (ret, params) in decl.items():
+        res, args = _lib.SIGNATURES[name]
+        assert len(args) == len(params), (name, len(args), params)
+        for i, (a, p) in enumerate(zip(args, params)):
+            assert _matches(a, p), (name, i, a, p)
+        assert _matches(res, ret) or (ret == "char*" and res is C.c_char_p), (name, res, ret)
+
+
 def test_version_and_state_size():
     from hastycucompute_b200 import _lib
     lib = _lib.load()
