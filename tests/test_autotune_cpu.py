@@ -4,7 +4,6 @@ without timing anything."""
 import json
 
 import numpy as np
-import pytest
 import torch
 
 from hastycucompute_b200 import autotune

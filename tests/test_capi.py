@@ -4,7 +4,6 @@ import ctypes as C
 import re
 from pathlib import Path
 
-import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 

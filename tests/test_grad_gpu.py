@@ -59,7 +59,6 @@ def _interp64(plan, pts, g):
 @pytest.mark.parametrize("nmodes,w,T", [((12, 14, 10), 6, 3), ((32, 24), 4, 5), ((40,), 6, 2), ((16, 16, 16), 8, 12)])
 def test_type2_coordinate_gradient(cuda, nmodes, w, T):
     import torch
-    import hastycucompute_b200 as hb
     from hastycucompute_b200 import autograd as ag
     rng = np.random.default_rng(len(nmodes) * 10 + w)
     dim, M = len(nmodes), 1500

@@ -1,6 +1,5 @@
 """Toeplitz kernel build, fused multiplication (all reference flag combinations) and the SENSE
 normal operator on the GPU through the C ABI, against the oracle. Bar: relative L2 <= 1e-5."""
-import itertools
 
 import numpy as np
 import pytest

@@ -4,7 +4,7 @@ peak memory with checkpointing."""
 import numpy as np
 import pytest
 
-from helpers import crand, rand_coords, relerr, to_dev, to_np
+from helpers import rand_coords, relerr, to_dev
 
 
 def _setup(cuda, F=2, shape=(16, 16, 16), C=3):

@@ -8,7 +8,6 @@ previous call's contents), and that a problem larger than its fixed workspace is
 anything runs. The file name sorts last so a run that stops at the first failure has run every
 other test first.
 """
-import ctypes as C
 
 import numpy as np
 import pytest
