@@ -61,7 +61,7 @@ double kb_fit(KbPoly* p, int w, double beta) {
         worst = 0.0;
         for (int d = 0; d < w; ++d) {
             // Chebyshev coefficients of f(s) = phi(d - w/2 + (s+1)/2) on s in [-1,1].
-            double fk[kMaxDeg + 1], a[kMaxDeg + 1];
+            double fk[kMaxDeg + 1], a[kMaxDeg + 1] = {0};
             for (int k = 0; k < n; ++k) {
                 double s = std::cos(M_PI * (k + 0.5) / n);
                 fk[k] = kb_phi((double)d - 0.5 * w + 0.5 * (s + 1.0), w, beta);
