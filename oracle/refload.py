@@ -69,7 +69,8 @@ def multiplication(inp, out, kernel, mult1=None, mult2=None, io_mult=0, in_m1=1,
     for b in range(B):
         scratch[...] = 0
         launch(b, -1)  # load batch b into scratch[0:N)
-        conv = np.fft.ifftn(np.fft.fftn(scratch[data_region], s=scratch.shape) * K)
+        axes = tuple(range(scratch.ndim))
+        conv = np.fft.ifftn(np.fft.fftn(scratch[data_region], s=scratch.shape, axes=axes) * K, axes=axes)
         scratch[...] = conv.astype(np.complex64)
         launch(-1, b)  # store batch b from scratch[N-1 : 2N-1)
     return res
