@@ -17,7 +17,8 @@ time.
 
 --impl reference times the reference-side CPU implementation (the oracle restatement of the
 straight Toeplitz SENSE normal operator, cpp/corelib/lib/fft/nufft.cppm:448-479 +
-cpp/corelib/lib/mri/normal.cppm:65-88, multithreaded FFT) on rank 0.
+cpp/corelib/lib/mri/normal.cppm:65-88, multithreaded FFT; one full apply over every coil per
+step, with the Toeplitz kernel built by the FP64 gridding oracle) on rank 0.
 """
 from __future__ import annotations
 
@@ -171,28 +172,31 @@ def max_over_ranks(v: float, world: int, device) -> float:
 # reference arm: CPU restatement on the host cores
 
 def run_reference(args, wl_name: str):
+    """The reference-side CPU path, timed on the host cores: the Toeplitz kernel built by the FP64
+    gridding oracle (cpp/corelib/lib/fft/nufft.cppm:386-441 restated, untimed set-up), then per
+    step one full straight Toeplitz SENSE normal apply over every coil (nufft.cppm:448-479 +
+    cpp/corelib/lib/mri/normal.cppm:65-88) in complex64 with torch's multithreaded CPU FFT."""
     world, rank, _ = dist_setup(False)
     if rank != 0:
         return 0
+    import torch
     from oracle import toeplitz as otp
 
     wl = make_workload_cpu_only(wl_name)
     shape, C = wl["shape"], wl["C"]
     cores = len(os.sched_getaffinity(0))
-    rng = np.random.default_rng(7)
-    # a random Hermitian-structured kernel stands in for the built one: the apply's cost does
-    # not depend on its values
-    K = (rng.standard_normal(tuple(2 * s for s in shape)) + 1j * rng.standard_normal(tuple(2 * s for s in shape))).astype(np.complex64)
-    coils_per_step = 1
+    torch.set_num_threads(cores)
+    t0 = time.perf_counter()
+    K = otp.toeplitz_kernel(list(wl["coords"]), shape, wl["dcf"], w=wl["w"]).astype(np.complex64)
+    t_kernel = time.perf_counter() - t0
     times = []
     for it in range(args.warmup + args.steps):
-        c0 = it % C
         t0 = time.perf_counter()
-        otp.sense_normal(wl["x"], wl["smaps"][c0:c0 + coils_per_step], K, workers=cores, dtype=np.complex64)
+        otp.sense_normal(wl["x"], wl["smaps"], K, dtype=np.complex64, fast=True)
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             times.append(dt)
-    per_apply = statistics.mean(times) * C / coils_per_step
+    per_apply = statistics.mean(times)
     value = 1.0 / per_apply
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "applies/s", "n_gpus": args.gpus,
@@ -200,8 +204,9 @@ def run_reference(args, wl_name: str):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(wl),
         "cpu_baseline": {"value": value, "unit": "applies/s", "cores": cores, "kind": "port",
-                         "sample": f"{coils_per_step} of {C} coils per step (straight Toeplitz SENSE normal, "
-                                   f"scipy FFT on {cores} threads), scaled to a full apply"},
+                         "sample": f"every step one full apply over all {C} coils (straight Toeplitz SENSE normal, "
+                                   f"complex64, torch CPU FFT on {cores} threads); Toeplitz kernel built by the FP64 "
+                                   f"gridding oracle in {t_kernel:.1f} s, untimed"},
         "e2e": {"value": value, "unit": "applies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -462,6 +467,14 @@ def bench_nufft(args, hb, _lib, coords, wl, dev, stream, hbm_peak):
     g_ref = nudft.type1_at(wl["coords"], y_np, shape, idx, sign=1)
     g_got = g[:1].cpu().numpy()[(slice(None),) + tuple(idx[:, i] for i in range(d))]
     res["type1"]["rel_err_vs_nudft"] = float(np.linalg.norm(g_got - g_ref) / np.linalg.norm(g_ref))
+    if not args.no_check:
+        # two of the transforms at full size against the FP64 gridding oracle (same kernel, width,
+        # upsampling; multithreaded C spreading / interpolation)
+        from oracle import gridding
+        res["type2"]["rel_err_vs_fp64_gridding_2_transforms"] = _rel(
+            y[:2].cpu().numpy(), gridding.nufft2(list(wl["coords"]), f_np, w=w))
+        res["type1"]["rel_err_vs_fp64_gridding_2_transforms"] = _rel(
+            g[:2].cpu().numpy(), gridding.nufft1(list(wl["coords"]), y[:2].cpu().numpy(), shape, w=w))
     p1.free()
     p2.free()
     return res
@@ -505,6 +518,15 @@ def bench_frames(args, hb, dev, stream, nframes=24, shape=(128, 128, 128), C=16,
     torch.cuda.synchronize()
     t_batched = e0.elapsed_time(e1) / 1e3
     xb = xb.clone()
+    acc = None
+    if not args.no_check:
+        # frame 0 of the batched recon against the FP64 oracle CG on its own straight operator
+        from oracle import cg as ocg, toeplitz as otp
+        Sn = S.cpu().numpy().astype(np.complex128)
+        Kn = Ks[0].cpu().numpy().astype(np.complex128)
+        x_ref, _ = ocg.conjugate_gradient(lambda v: otp.sense_normal(v, Sn, Kn, fast=True), b[0].cpu().numpy(),
+                                          np.zeros(shape, np.complex64), iters, tol=0.0)
+        acc = _rel(xb[0].cpu().numpy(), x_ref)
     del solver, op
     torch.cuda.empty_cache()
     # per-frame loop with the plain operator (NUFFT type 2 then type 1 per apply): the frame's
@@ -529,6 +551,7 @@ def bench_frames(args, hb, dev, stream, nframes=24, shape=(128, 128, 128), C=16,
             "batched_recons_per_s": round(nframes / t_batched, 3), "batched_s": round(t_batched, 3),
             "looped_recons_per_s": round(nframes / t_loop, 3), "looped_s": round(t_loop, 3),
             "speedup": round(t_loop / t_batched, 2), "batched_vs_looped_rel_diff": diff,
+            "batched_frame0_rel_err_vs_fp64_oracle_cg": acc,
             "toeplitz_kernels_s": round(t_kernels, 3), "graph_captured": True}
 
 
@@ -592,6 +615,18 @@ def bench_configs(args, hb, dev, stream):
     res["config0"] = {"workload": "64^3, 8 coils, golden-means radial 1024 x 128, KB w=4",
                       "aha_applies_per_s": round(1e3 / aha_ms, 1), "type2_msamp_per_s": t2r,
                       "type1_msamp_per_s": t1r, "cg10_recons_per_s": round(1e3 / cg_ms, 2)}
+    if not args.no_check:
+        # the timed recon against the FP64 oracle CG (cpp/corelib/lib/op/cg.cppm:122-184 restated) on
+        # the FP64 straight Toeplitz SENSE normal operator with the same kernel
+        from oracle import cg as ocg, toeplitz as otp
+        xs = solver.solve(torch.zeros_like(x), b).cpu().numpy()
+        Sn = S.cpu().numpy().astype(np.complex128)
+        Kn = K.cpu().numpy().astype(np.complex128)
+        x_ref, _ = ocg.conjugate_gradient(lambda v: otp.sense_normal(v, Sn, Kn, fast=True), b.cpu().numpy(),
+                                          np.zeros(shape, np.complex64), 10, tol=0.0)
+        res["config0"]["cg10_rel_err_vs_fp64_oracle"] = _rel(xs, x_ref)
+        res["config0"]["aha_rel_err_vs_fp64_oracle"] = _rel(b.cpu().numpy(), otp.sense_normal(
+            x.cpu().numpy(), Sn, Kn, fast=True))
     del solver, op, K, S
     # ---- config 3 --------------------------------------------------------------------------------
     shape, C, ninter, ns = (256, 256), 12, 32, 2048
@@ -619,9 +654,32 @@ def bench_configs(args, hb, dev, stream):
     loss_ms = timed(step, 3)
     res["config3"] = {"workload": "2-D 256^2, 12 coils, 32 variable-density spirals x 2048, KB w=4",
                       "type2_msamp_per_s": t2r, "type1_msamp_per_s": t1r,
-                      "loss_forward_backward_ms": round(loss_ms, 2),
-                      "gradient_check": "tests/test_grad_gpu.py: 64 coordinates and 16 pixels vs central "
-                                        "differences (h = 1e-4) of the FP64 NUDFT loss, <= 1e-3"}
+                      "loss_forward_backward_ms": round(loss_ms, 2)}
+    if not args.no_check:
+        # gradients of the timed loss against the FP64 gridding oracle of the same loss: the image
+        # gradient exactly, 16 coordinate gradients by central differences (h = 1e-4)
+        from oracle.loss import SenseLoss
+        xg = x0.clone().requires_grad_(True)
+        kg = kk.clone().requires_grad_(True)
+        r = ag.nufft_forward(S * xg[None], kg, pair) - y
+        gimg = (torch.conj(S) * ag.nufft_adjoint(r, kg, pair)).sum(0)
+        k3 = kg.reshape(2, ninter, ns)
+        slew = ((k3[:, :, 2:] - 2 * k3[:, :, 1:-1] + k3[:, :, :-2]) ** 2).sum()
+        ((gimg.abs() ** 2).sum() + 1e-3 * slew).backward()
+        ol = SenseLoss(S.cpu().numpy(), y.cpu().numpy(), k0, w=w, lam=1e-3, interleaves=ninter)
+        ol.setup(x0.cpu().numpy())
+        rng = np.random.default_rng(4)
+        M3 = k0.shape[1]
+        picks = []
+        while len(picks) < 16:
+            a, j = divmod(int(rng.integers(0, 2 * M3)), M3)
+            if (a, j) not in picks and not ol.crosses_cell(a, j, 1e-4):
+                picks.append((a, j))
+        gk = kg.grad.cpu().numpy().astype(np.float64)
+        fd = np.array([ol.coord_fd(a, j, 1e-4) for a, j in picks])
+        res["config3"]["image_grad_rel_err_vs_fp64_oracle"] = _rel(xg.grad.cpu().numpy(), ol.image_grad())
+        res["config3"]["coord_grad_rel_err_vs_central_differences"] = _rel(np.array([gk[a, j] for a, j in picks]), fd)
+        res["config3"]["coord_grad_check"] = "16 coordinates, h = 1e-4, FP64 gridding oracle loss (64 in the GPU tests)"
     del pair, S
     torch.cuda.empty_cache()
     # ---- config 4 --------------------------------------------------------------------------------
@@ -635,6 +693,11 @@ def bench_configs(args, hb, dev, stream):
     ob = torch.empty_like(xt)
     apply_ms = timed(lambda: op4.apply(xt, ob), 5)
     b4 = op4(xt)
+    acc4 = None
+    if not args.no_check:
+        from oracle import toeplitz as otp
+        acc4 = _rel(b4[0].cpu().numpy(), otp.sense_normal(xt[0].cpu().numpy(), S.cpu().numpy().astype(np.complex128),
+                                                          Ks[0].cpu().numpy().astype(np.complex128), fast=True))
     net = UnrolledCG(op4, iterations=10, step_init=0.9, lam_init=0.01, checkpoint=True).to(dev)
 
     def fb():
@@ -653,11 +716,18 @@ def bench_configs(args, hb, dev, stream):
                       "aha_applies_per_s_per_volume": round(F * 1e3 / apply_ms, 1),
                       "unrolled_forward_backward_ms": round(fb_ms, 1),
                       "peak_hbm_gb": round(peak / 1e9, 2), "resident_before_gb": round(base / 1e9, 2),
-                      "scalar_gradient_check": "tests/test_unrolled_gpu.py: steps and weights vs central "
-                                               "differences, <= 1e-3"}
+                      "aha_rel_err_vs_fp64_oracle": acc4,
+                      "scalar_gradient_check": "tests/test_configs_gpu.py: the 20 learnable scalars at this size "
+                                               "vs central differences (h = 1e-2), <= 1e-3"}
     del net, op4, Ks, S
     torch.cuda.empty_cache()
     return res
+
+
+def _rel(a, b) -> float:
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
 
 
 def check_accuracy(hb, wl, K, dev):
@@ -671,26 +741,29 @@ def check_accuracy(hb, wl, K, dev):
     Kn = K.cpu().numpy().astype(np.complex128)
     cores = len(os.sched_getaffinity(0))
     ref = otp.sense_normal(wl["x"], sub, Kn, workers=cores)
+    K_ref = otp.toeplitz_kernel(list(wl["coords"]), wl["shape"], wl["dcf"], w=wl["w"])
     return {"aha_rel_err_vs_fp64_oracle": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
-            "coils_checked": 2}
+            "coils_checked": 2, "toeplitz_kernel_rel_err_vs_fp64_oracle": _rel(Kn, K_ref)}
 
 
 def cpu_baseline(wl, K):
+    """Two full straight Toeplitz SENSE normal applies (every coil) on the host cores with the
+    kernel the GPU built, complex64, torch's CPU FFT on all cores; the mean is reported."""
     from oracle import toeplitz as otp
     import torch
     cores = len(os.sched_getaffinity(0))
+    torch.set_num_threads(cores)
     Kn = K.cpu().numpy()
     C = wl["C"]
-    # bounded sample: 1 coil, twice; scaled to a full apply
     times = []
-    for c0 in range(2):
+    for _ in range(2):
         t0 = time.perf_counter()
-        otp.sense_normal(wl["x"], wl["smaps"][c0:c0 + 1], Kn, workers=cores, dtype=np.complex64)
+        otp.sense_normal(wl["x"], wl["smaps"], Kn, dtype=np.complex64, fast=True)
         times.append(time.perf_counter() - t0)
-    per_apply = min(times) * C
+    per_apply = statistics.mean(times)
     return {"value": round(1.0 / per_apply, 5), "unit": "applies/s", "cores": cores, "kind": "port",
-            "sample": f"1 of {C} coils (straight Toeplitz SENSE normal, scipy FFT on {cores} threads), "
-                      f"scaled to a full apply"}
+            "sample": f"2 full applies over all {C} coils (straight Toeplitz SENSE normal, complex64, torch CPU "
+                      f"FFT on {cores} threads), mean {per_apply:.2f} s per apply"}
 
 
 def main(argv=None):

@@ -17,6 +17,8 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
+
 #include "nufft.cuh"
 #include "ops.cuh"
 
@@ -723,24 +725,60 @@ static __device__ __align__(256) float2 g_noalloc_ws[kNoAllocWsBytes / sizeof(fl
 static __device__ __align__(256) float2 g_noalloc_tw[3 * kNoAllocMaxLen];
 
 struct NoAllocDevice {
+    int dev = -1;
+    unsigned long long ctx_id = 0;  // driver context id the addresses belong to
     float2* ws = nullptr;
     float2* tw = nullptr;
 };
 static std::mutex g_noalloc_mu;
 static std::vector<NoAllocDevice> g_noalloc_dev;
 
-// Device addresses of the two arrays for the current device, looked up once per device.
+// Unique id of the current driver context (cuCtxGetId, reached through the runtime's driver
+// entry-point query so the library does not link libcuda). A device reset destroys the primary
+// context and the next runtime call creates a new one with a new id, at which point the module
+// holding the arrays is loaded again at new addresses.
+static int current_context_id(unsigned long long* id) {
+    using PfnGetCurrent = CUresult (*)(CUcontext*);
+    using PfnGetId = CUresult (*)(CUcontext, unsigned long long*);
+    static PfnGetCurrent get_current = nullptr;
+    static PfnGetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (PfnGetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (PfnGetId)f;
+    });
+    HB_REQUIRE(get_current && get_id, HB_ERR_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId unavailable");
+    CUcontext ctx = nullptr;
+    HB_REQUIRE(get_current(&ctx) == CUDA_SUCCESS && ctx != nullptr, HB_ERR_CUDA, "no current CUDA context");
+    HB_REQUIRE(get_id(ctx, id) == CUDA_SUCCESS, HB_ERR_CUDA, "cuCtxGetId failed");
+    return HB_OK;
+}
+
+// Device addresses of the two arrays for the current device, looked up once per device and
+// context with that device current.
 static int noalloc_addresses(NoAllocDevice* out) {
     int dev = 0;
     HB_CUDA(cudaGetDevice(&dev));
+    HB_CUDA(cudaSetDevice(dev));  // initialises the device's primary context and makes it current
+    unsigned long long ctx_id = 0;
+    HB_TRY(current_context_id(&ctx_id));
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if ((int)g_noalloc_dev.size() <= dev) g_noalloc_dev.resize(dev + 1);
     NoAllocDevice& d = g_noalloc_dev[dev];
-    if (d.ws == nullptr || d.tw == nullptr) {
+    if (d.ws == nullptr || d.tw == nullptr || d.dev != dev || d.ctx_id != ctx_id) {
         void* ws = nullptr;
         void* tw = nullptr;
         HB_CUDA(cudaGetSymbolAddress(&ws, g_noalloc_ws));
         HB_CUDA(cudaGetSymbolAddress(&tw, g_noalloc_tw));
+        d.dev = dev;
+        d.ctx_id = ctx_id;
         d.ws = (float2*)ws;
         d.tw = (float2*)tw;
     }
@@ -784,7 +822,8 @@ int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const vo
     if (need > kNoAllocWsBytes) {
         set_error("hb_sense_normal_noalloc: problem needs " + std::to_string(need) +
                   " bytes of workspace, the fixed array holds " + std::to_string(kNoAllocWsBytes) +
-                  " (6 * prod(N) * ncoils * 8 bytes must fit)");
+                  (t.dim == 3 ? " (3-D: 6 * prod(N) * ncoils * 8 bytes must fit)"
+                              : " (2-D: 2 * prod(N) * ncoils * 8 bytes must fit)"));
         return HB_ERR_WORKSPACE;
     }
     for (int ax = 0; ax < 3; ++ax)
@@ -803,7 +842,7 @@ int sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const vo
     float2* W2 = d.ws + (size_t)N0 * N1 * L2 * B;
     const int64_t E2 = (int64_t)L2 * B;
     {
-        OpToepIn op{S, (const float2*)x, nullptr, HB_MULT_MULT, HB_MULT_NONE, W1, N2, t.n, E2, B, 0};
+        OpToepInSense op{{S, (const float2*)x, nullptr, HB_MULT_MULT, HB_MULT_NONE, W1, N2, t.n, E2, B, 0}};
         HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, (int)N2, 0, L2, 0, 0, 0, s, "noalloc P1"));
     }
     if (t.dim == 3) {

@@ -203,11 +203,12 @@ int hb_transform_toeplitz_kernels(int dim, const int64_t* kernel_shape, int64_t 
  * allocations, a driver layer handing out fixed buffers, code running where cudaMalloc is off
  * limits. It allocates nothing: the workspace (32 MiB) and the FFT twiddle tables sit in fixed
  * device arrays inside this library, which every GPU that loads it keeps until exit. Limits:
- * 6 * prod(N) * ncoils * 8 bytes <= 32 MiB (else HB_ERR_WORKSPACE, nothing launched) and
- * 2N <= 4096 per axis. The first call on a device looks up the arrays' device addresses; make
- * that first call before any stream capture. All calls share the arrays, so calls that overlap
- * on the GPU (different streams, threads or processes sharing a context) race: serialise them.
- * Result as hb_sense_normal. */
+ * the workspace need, 3-D 6 * prod(N) * ncoils * 8 bytes and 2-D 2 * prod(N) * ncoils * 8
+ * bytes, must be <= 32 MiB (else HB_ERR_WORKSPACE, nothing launched), and 2N <= 4096 per axis.
+ * The first call on a device (and the first after a device reset, which reloads the arrays at
+ * new addresses) looks up the arrays' device addresses; make that first call before any stream
+ * capture. All calls share the arrays, so calls that overlap on the GPU (different streams,
+ * threads or processes sharing a context) race: serialise them. Result as hb_sense_normal. */
 int hb_sense_normal_noalloc(int dim, const int64_t* shape, int64_t ncoils, const void* x,
                             const void* smaps, const void* kernel, void* out, void* stream);
 

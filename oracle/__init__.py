@@ -20,7 +20,6 @@ Contents
                  (cpp/corelib/lib/fft/kernels/toeplitz_load_{2D,3D}.cu), compiled for the CPU by
                  ``oracle/ref_load/Makefile`` into ``oracle/_ref/`` and driven from Python.
 - ``cg``         conjugate gradient following cpp/corelib/lib/op/cg.cppm:122-184.
-- ``phantoms``   seeded synthetic inputs (images, coil maps, trajectories, DCF).
 
 Parity status: the reference publishes no golden vectors or fixtures for this path, and its
 NUFFT is the third-party finufft/cufinufft (pinned only to ``master`` in CMakeLists.txt:175-181,

@@ -12,17 +12,20 @@ Restated here with the Kaiser-Bessel kernel of ``oracle.kb``:
 
 Coordinates are folded to the fine grid with float32 arithmetic exactly as the device does, so
 both pick the same first cell i0 = ceil(u - w/2) for every point; the kernel is then evaluated in
-FP64.
+FP64. Spreading and interpolation run in the multithreaded C restatement (``oracle.cgrid``) when
+it is built, else in numpy (``backend`` forces one); the fine-grid FFT runs in scipy, FP64.
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
-from . import kb
+from . import cgrid, kb
 
 
 class GridPlan:
-    def __init__(self, nmodes, w: int, sigma: float = 2.0, sign: int = 1):
+    def __init__(self, nmodes, w: int, sigma: float = 2.0, sign: int = 1, backend: str = "auto"):
         self.nmodes = tuple(int(n) for n in nmodes)
         self.dim = len(self.nmodes)
         self.w = int(w)
@@ -30,6 +33,9 @@ class GridPlan:
         self.sign = int(sign)
         self.beta = kb.beta(self.w, self.sigma)
         self.nf = kb.fine_grid(self.nmodes, self.w, self.sigma)
+        if backend == "auto":
+            backend = "c" if cgrid.available() else "numpy"
+        self.backend = backend
 
     # -- coordinates --------------------------------------------------------------------------
     def fold(self, x, nf: int):
@@ -76,6 +82,8 @@ class GridPlan:
         return idx, wt  # [M, w^d]
 
     def spread(self, coords, c):
+        if self.backend == "c":
+            return cgrid.spread(self.nf, self.w, self.beta, coords, c)
         c = np.asarray(c, dtype=np.complex128)
         idx, wt = self._flat_taps(coords)
         n = int(np.prod(self.nf))
@@ -87,17 +95,21 @@ class GridPlan:
         return out.reshape(c.shape[0], *self.nf)
 
     def interp(self, coords, g):
+        if self.backend == "c":
+            return cgrid.interp(self.nf, self.w, self.beta, coords, np.asarray(g).reshape(g.shape[0], *self.nf))
         g = np.asarray(g, dtype=np.complex128).reshape(g.shape[0], -1)
         idx, wt = self._flat_taps(coords)
         return np.einsum("tmk,mk->tm", g[:, idx], wt, optimize=True)
 
     # -- FFT over the fine grid ------------------------------------------------------------------
     def _fft(self, a, sign: int):
+        import scipy.fft as sf
         axes = tuple(range(1, self.dim + 1))
+        workers = len(os.sched_getaffinity(0))
         if sign < 0:
-            return np.fft.fftn(a, axes=axes)
+            return sf.fftn(a, axes=axes, workers=workers)
         n = int(np.prod(self.nf))
-        return np.fft.ifftn(a, axes=axes) * n
+        return sf.ifftn(a, axes=axes, workers=workers) * n
 
     def _mode_index(self, axis: int) -> np.ndarray:
         N, nf = self.nmodes[axis], self.nf[axis]
@@ -129,9 +141,9 @@ class GridPlan:
         return self.interp(coords, g)
 
 
-def nufft1(coords, c, nmodes, w: int, sigma: float = 2.0, sign: int = 1):
-    return GridPlan(nmodes, w, sigma, sign).type1(coords, c)
+def nufft1(coords, c, nmodes, w: int, sigma: float = 2.0, sign: int = 1, backend: str = "auto"):
+    return GridPlan(nmodes, w, sigma, sign, backend).type1(coords, c)
 
 
-def nufft2(coords, f, w: int, sigma: float = 2.0, sign: int = -1):
-    return GridPlan(f.shape[1:], w, sigma, sign).type2(coords, f)
+def nufft2(coords, f, w: int, sigma: float = 2.0, sign: int = -1, backend: str = "auto"):
+    return GridPlan(f.shape[1:], w, sigma, sign, backend).type2(coords, f)

@@ -28,9 +28,15 @@ def toeplitz_kernel(coords, shape, weights=None, w: int = 6, sigma: float = 2.0,
         red = nudft.type1(coords, nud, nm, sign=1)[0]
     else:
         red = gridding.nufft1(coords, nud, nm, w=w, sigma=sigma, sign=1)[0]
+    import os
+
+    import scipy.fft as sf
     k = np.zeros(tuple(2 * s for s in shape), dtype=np.complex128)
     k[tuple(slice(0, m) for m in nm)] = red
-    return np.fft.fftn(k) / float(np.prod(shape))
+    del red
+    k = sf.fftn(k, workers=len(os.sched_getaffinity(0)), overwrite_x=True)
+    k /= float(np.prod(shape))
+    return k
 
 
 def toeplitz_multiply(inout, kernel, workers: int | None = None, dtype=np.complex128):
@@ -52,6 +58,28 @@ def toeplitz_multiply(inout, kernel, workers: int | None = None, dtype=np.comple
         mid = mid * kernel[None]
         mid = np.fft.ifftn(mid, axes=axes)
     return mid[(slice(None),) + tuple(slice(s - 1, 2 * s - 1) for s in shape)]
+
+
+def toeplitz_multiply_torch(inout, kernel, dtype=np.complex128, chunk: int = 4):
+    """:func:`toeplitz_multiply` evaluated with torch's multithreaded CPU FFT (the same straight
+    pad / transform / multiply / inverse / crop sequence, in FP64 by default), ``chunk`` batches at
+    a time; for full configuration sizes. Returns a numpy array."""
+    import torch
+    inout = np.asarray(inout)
+    shape = inout.shape[1:]
+    d = len(shape)
+    tdt = torch.complex128 if dtype == np.complex128 else torch.complex64
+    K = torch.from_numpy(np.ascontiguousarray(kernel)).to(tdt)
+    out = np.empty(inout.shape, dtype=dtype)
+    dims = tuple(range(1, d + 1))
+    crop = (slice(None),) + tuple(slice(n - 1, 2 * n - 1) for n in shape)
+    for b0 in range(0, inout.shape[0], chunk):
+        v = torch.from_numpy(np.ascontiguousarray(inout[b0:b0 + chunk])).to(tdt)
+        v = torch.fft.fftn(v, s=tuple(2 * n for n in shape), dim=dims)
+        v *= K
+        v = torch.fft.ifftn(v, dim=dims)
+        out[b0:b0 + chunk] = v[crop].numpy()
+    return out
 
 
 def _m(a, b, t):
@@ -83,10 +111,14 @@ def toeplitz_multiplication(inp, out, kernel, mult1=None, mult2=None, io_mult=NO
     return v
 
 
-def sense_normal(x, smaps, kernel, workers: int | None = None, dtype=np.complex128):
+def sense_normal(x, smaps, kernel, workers: int | None = None, dtype=np.complex128, fast: bool = False):
+    """``fast`` evaluates the same convolution by :func:`toeplitz_multiply_torch`."""
     x = np.asarray(x, dtype=dtype)
     s = np.asarray(smaps, dtype=dtype)
-    v = toeplitz_multiply(s * x[None], kernel, workers=workers, dtype=dtype)
+    if fast:
+        v = toeplitz_multiply_torch(s * x[None], kernel, dtype=dtype)
+    else:
+        v = toeplitz_multiply(s * x[None], kernel, workers=workers, dtype=dtype)
     return np.sum(np.conj(s) * v, axis=0)
 
 

@@ -3,10 +3,12 @@
 It serves callers that cannot allocate device memory (a runtime embedded in another framework
 that owns every allocation, a driver layer that only hands out fixed buffers): its workspace and
 twiddle tables are fixed device arrays inside the library. This file checks it through the C ABI
-against the allocating entry point hb_sense_normal, on two calls in a row (the arrays keep the
-previous call's contents), and that a problem larger than its fixed workspace is refused before
-anything runs. The file name sorts last so a run that stops at the first failure has run every
-other test first.
+against the allocating entry point hb_sense_normal and against the FP64 oracle of the SENSE
+normal operator (NORMAL_T_T1_OP, cpp/corelib/lib/mri/normal.cppm:65-88), on two calls in a row
+(the arrays keep the previous call's contents); that a second call changes neither the device's
+free memory nor torch's allocator; and that a problem larger than its fixed workspace is refused
+before anything runs. The file name sorts last so a run that stops at the first failure has run
+every other test first.
 """
 
 import numpy as np
@@ -30,23 +32,50 @@ def _call(name, shape, C_, x, S, Kt, out, ws=None):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("shape,C_", [((16, 20, 24), 4), ((64, 80), 8), ((32, 32, 32), 3)])
-def test_noalloc_matches_allocating_entry_twice(cuda, shape, C_):
+def test_noalloc_matches_allocating_entry_and_oracle_twice(cuda, shape, C_):
     import torch
     import hastycucompute_b200 as hb
     from hastycucompute_b200 import synthetic, toeplitz as tp
+    from oracle import toeplitz as otp
     rng = np.random.default_rng(C_)
-    S = to_dev(synthetic.coil_maps(C_, shape), cuda)
-    K = to_dev(crand(rng, *[2 * s for s in shape]), cuda)
-    Kt = hb.transform_toeplitz_kernel(K)
+    Sn = synthetic.coil_maps(C_, shape)
+    S = to_dev(Sn, cuda)
+    Kn = crand(rng, *[2 * s for s in shape])
+    Kt = hb.transform_toeplitz_kernel(to_dev(Kn, cuda))
     ws = tp.make_workspace(shape, C_, cuda)
     for call in range(2):
-        x = to_dev(crand(rng, *shape), cuda)
+        xn = crand(rng, *shape)
+        x = to_dev(xn, cuda)
         ref = torch.empty_like(x)
         got = torch.full_like(x, float("nan"))
         _call("hb_sense_normal", shape, C_, x, S, Kt, ref, ws)
         _call("hb_sense_normal_noalloc", shape, C_, x, S, Kt, got)
         torch.cuda.synchronize()
         assert relerr(to_np(got), to_np(ref)) <= TOL, f"call {call}"
+        oracle = otp.sense_normal(xn, Sn, Kn.astype(np.complex128))
+        assert relerr(to_np(got), oracle) <= TOL, f"call {call} vs oracle"
+
+
+@pytest.mark.gpu
+def test_noalloc_second_call_allocates_nothing(cuda):
+    import torch
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import synthetic
+    shape, C_ = (24, 24, 24), 4
+    rng = np.random.default_rng(11)
+    S = to_dev(synthetic.coil_maps(C_, shape), cuda)
+    Kt = hb.transform_toeplitz_kernel(to_dev(crand(rng, *[2 * s for s in shape]), cuda))
+    x = to_dev(crand(rng, *shape), cuda)
+    outs = [torch.empty_like(x) for _ in range(2)]
+    _call("hb_sense_normal_noalloc", shape, C_, x, S, Kt, outs[0])  # loads the module and its arrays
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(cuda)[0]
+    alloc0, reserved0 = torch.cuda.memory_allocated(cuda), torch.cuda.memory_reserved(cuda)
+    _call("hb_sense_normal_noalloc", shape, C_, x, S, Kt, outs[1])
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(cuda)[0] == free0
+    assert (torch.cuda.memory_allocated(cuda), torch.cuda.memory_reserved(cuda)) == (alloc0, reserved0)
+    assert relerr(to_np(outs[1]), to_np(outs[0])) == 0.0
 
 
 @pytest.mark.gpu
