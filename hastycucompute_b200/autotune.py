@@ -1,10 +1,13 @@
-"""Spreading autotuner: picks the warp cell-block shape and the points per spread subproblem for a
-given problem by timing type-1 plans on the device, and caches the choice as JSON.
+"""Spreading autotuner: picks the spreading kernel, its cell block and the points per spread
+subproblem for a given problem by timing type-1 plans on the device, and caches the choice as JSON.
 
 Search space (all exact, all give the same result up to float rounding):
-- the 32-cell block each warp owns inside a spread tile: 3-D tiles are 8x8x8, so any
-  (bz, by, bx) with bz*by*bx = 32 and each edge dividing 8; 2-D tiles are 16x32;
-- points per subproblem (how dense tiles are split across CTAs): 1024 .. 8192.
+- the kernel: transforms on the lanes (each thread owns 4 rows x 8 cells of one transform; dense
+  tiles go to thread-block clusters of 2/4/8 CTAs) or cells on the lanes (each thread owns one
+  cell; dense tiles as extra subproblems);
+- for cells on the lanes, the 32-cell block each warp owns inside a spread tile: 3-D tiles are
+  8x8x8, so any (bz, by, bx) with bz*by*bx = 32 and each edge dividing 8; 2-D tiles are 16x32;
+- points per subproblem (when a tile is dense enough to split): 256 .. 8192.
 
 Cache key: dimensionality, modes, transforms, kernel width, number of points and a coarse
 density signature of the trajectory (quartiles of |k|), so the same trajectory family reuses the
@@ -24,6 +27,7 @@ from .nufft import NufftOpts, NufftPlan, NufftType
 BLOCKS_3D = [(2, 4, 4), (4, 4, 2), (2, 2, 8), (4, 2, 4), (1, 4, 8), (8, 2, 2), (2, 8, 2)]
 BLOCKS_2D = [(1, 4, 8), (1, 8, 4), (1, 2, 16), (1, 16, 2), (1, 1, 32)]
 MAXP = [1024, 2048, 4096, 8192]
+MAXP_TRANSFORMS = [256, 512, 1024, 2048, 4096]
 
 
 def cache_path() -> Path:
@@ -59,8 +63,9 @@ def _store(d: dict) -> None:
 
 def tune_spread(nmodes: Sequence[int], ntransf: int, coords: Sequence[torch.Tensor], kernel_width: int,
                 reps: int = 3, use_cache: bool = True, candidates: Optional[list] = None) -> dict:
-    """Times type-1 executes over the search space; returns {"block", "max_candidates", "ms",
-    "timings"} for the fastest and stores it in the cache."""
+    """Times type-1 executes over the search space; returns {"kernel", "block", "max_candidates",
+    "ms", "timings"} for the fastest and stores it in the cache. ``candidates`` entries are
+    (kernel, block, max_candidates)."""
     nmodes = tuple(int(n) for n in nmodes)
     key = _key(nmodes, ntransf, kernel_width, coords)
     cache = _load() if use_cache else {}
@@ -69,14 +74,16 @@ def tune_spread(nmodes: Sequence[int], ntransf: int, coords: Sequence[torch.Tens
     dev = coords[0].device
     blocks = BLOCKS_3D if len(nmodes) == 3 else BLOCKS_2D
     if candidates is None:
-        candidates = [(b, m) for b in blocks for m in MAXP]
+        candidates = [("transforms", blocks[0], m) for m in MAXP_TRANSFORMS]
+        candidates += [("cells", b, m) for b in blocks for m in MAXP]
     M = coords[0].shape[0]
     data = torch.randn((ntransf, M), dtype=torch.complex64, device=dev)
     out = torch.empty((ntransf, *nmodes), dtype=torch.complex64, device=dev)
     timings = []
-    for block, maxp in candidates:
+    for kernel, block, maxp in candidates:
         plan = NufftPlan(NufftType.TYPE_1, NufftOpts(nmodes=nmodes, ntransf=ntransf, kernel_width=kernel_width))
         try:
+            plan.set_spread_kernel(kernel)
             plan.set_spread_tuning(maxp, block)
         except Exception:
             plan.free()
@@ -90,11 +97,11 @@ def tune_spread(nmodes: Sequence[int], ntransf: int, coords: Sequence[torch.Tens
             plan.execute(data, out)
         e1.record()
         torch.cuda.synchronize(dev)
-        timings.append((e0.elapsed_time(e1) / reps, list(block), int(maxp)))
+        timings.append((e0.elapsed_time(e1) / reps, kernel, list(block), int(maxp)))
         plan.free()
-    timings.sort()
-    best = {"block": timings[0][1], "max_candidates": timings[0][2], "ms": round(timings[0][0], 4),
-            "timings": [[round(t, 4), b, m] for t, b, m in timings]}
+    timings.sort(key=lambda r: r[0])
+    best = {"kernel": timings[0][1], "block": timings[0][2], "max_candidates": timings[0][3],
+            "ms": round(timings[0][0], 4), "timings": [[round(t, 4), k, b, m] for t, k, b, m in timings]}
     if use_cache:
         cache = _load()
         cache[key] = best
@@ -104,4 +111,5 @@ def tune_spread(nmodes: Sequence[int], ntransf: int, coords: Sequence[torch.Tens
 
 def apply(plan: NufftPlan, choice: dict) -> None:
     """Applies a tuner choice to a plan (before its setpts)."""
+    plan.set_spread_kernel(choice.get("kernel", "auto"))
     plan.set_spread_tuning(int(choice["max_candidates"]), tuple(choice["block"]))

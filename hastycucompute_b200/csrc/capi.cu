@@ -126,6 +126,16 @@ int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block
     })
 }
 
+int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind) {
+    HB_GUARD({
+        if (!plan) {
+            hb::set_error("plan is null");
+            return HB_ERR_INVALID_ARG;
+        }
+        return hb::plan_set_spread_kernel(&plan->p, kind);
+    })
+}
+
 int hb_nufft_coord_grad(hb_nufft_plan plan, const void* modes, const void* h, float* grad, void* stream) {
     HB_GUARD({
         if (!plan) {

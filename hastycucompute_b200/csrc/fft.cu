@@ -11,7 +11,7 @@ int fftlen_make(FftLen* f, int L) {
     f->nrad = 0;
     f->tw = nullptr;
     int rest = L;
-    const int order[6] = {8, 4, 2, 5, 3, 7};
+    const int order[8] = {8, 4, 2, 5, 3, 7, 11, 13};
     for (int r : order) {
         while (rest % r == 0 && rest > 1) {
             if (f->nrad >= kMaxRadices) {
@@ -23,7 +23,7 @@ int fftlen_make(FftLen* f, int L) {
         }
     }
     if (rest != 1) {
-        set_error("FFT length " + std::to_string(L) + " is not 2,3,5,7-smooth");
+        set_error("FFT length " + std::to_string(L) + " has a prime factor other than 2, 3, 5, 7, 11, 13");
         return HB_ERR_INVALID_ARG;
     }
     std::vector<float2> h(L);

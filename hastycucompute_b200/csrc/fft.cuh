@@ -2,7 +2,7 @@
 //
 // One "pass" transforms a 3-level array  X[a][l][e]  (a = outer batch, l = the transformed
 // axis, e = inner columns, contiguous) along l. A CTA takes A_blk outer x E_blk inner columns,
-// stages the L samples of each column in shared memory, runs Stockham radix-{2,3,4,5,7,8}
+// stages the L samples of each column in shared memory, runs Stockham radix-{2,3,4,5,7,8,11,13}
 // stages between two shared buffers, and writes back. Pruning is built into the pass:
 //   - only Lin input samples are read; sample l lands at FFT position (l + in_shift) mod L and
 //     every other position is zero (zero padding / centred modes without a padding pass);
@@ -13,6 +13,9 @@
 #pragma once
 
 #include <stdint.h>
+
+#include <type_traits>
+#include <utility>
 
 #include "common.cuh"
 #include "timing.cuh"
@@ -30,7 +33,7 @@ struct FftLen {
     float2* tw = nullptr;  // device, L entries, tw[m] = exp(-2 pi i m / L)
 };
 
-// Factorises L into radices 8,4,2,5,3,7 (an error if L has another prime factor) and
+// Factorises L into radices 8,4,2,5,3,7,11,13 (an error if L has another prime factor) and
 // uploads its twiddle table (synchronous cudaMalloc + cudaMemcpy).
 int fftlen_make(FftLen* f, int L);
 void fftlen_free(FftLen* f);
@@ -63,6 +66,44 @@ inline size_t pass_smem_bytes(const PassCfg& c, size_t extra_bytes) {
 }
 
 #ifdef __CUDACC__
+
+// ---- compile-time twiddles -----------------------------------------------------------------
+// W_R^m = exp(-2 pi i m / R) evaluated while compiling: the angle is reduced to [-pi, pi] and
+// sine / cosine are summed from their Taylor series in double (terms to x^31, error far below
+// float rounding), then rounded once to float. Exact quarter turns become swaps.
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+constexpr double ct_sin(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 16; ++k) {
+        term *= -x * x / (double)((2 * k) * (2 * k + 1));
+        sum += term;
+    }
+    return sum;
+}
+constexpr double ct_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 16; ++k) {
+        term *= -x * x / (double)((2 * k - 1) * (2 * k));
+        sum += term;
+    }
+    return sum;
+}
+template <int R, int M>
+constexpr double ct_angle() {
+    constexpr int m = ((M % R) + R) % R;
+    return kTwoPi * (double)(2 * m > R ? m - R : m) / (double)R;  // in [-pi, pi]
+}
+
+// Calls f(std::integral_constant<int, I>) for I = 0 .. N-1 (indices usable as constants).
+template <class F, int... I>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+    static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
 
 // ---- DFT codelets ----------------------------------------------------------------------
 // forward: y_s = sum_r x_r exp(-2 pi i r s / R); INV flips the sign of the exponent.
@@ -181,9 +222,45 @@ __device__ __forceinline__ void dft8(float2* v) {
     v[7] = csub(e3, w3o);
 }
 
+// Odd-prime DFT (11, 13) by the symmetric pairs t_j = x_j + x_{R-j}, u_j = x_j - x_{R-j}:
+//   y_k = x_0 + sum_j cos(2 pi jk/R) t_j -/+ i sum_j sin(2 pi jk/R) u_j, y_{R-k} with the other
+// sign (forward / inverse); every cosine and sine is a compile-time constant.
+template <int R, bool INV>
+__device__ __forceinline__ void dft_odd(float2* v) {
+    constexpr int H = (R - 1) / 2;
+    float2 t[H], u[H];
+#pragma unroll
+    for (int j = 1; j <= H; ++j) {
+        t[j - 1] = cadd(v[j], v[R - j]);
+        u[j - 1] = csub(v[j], v[R - j]);
+    }
+    const float2 x0 = v[0];
+    float2 sum = x0;
+#pragma unroll
+    for (int j = 0; j < H; ++j) sum = cadd(sum, t[j]);
+    static_for<H>([&](auto kk) {
+        constexpr int k = decltype(kk)::value + 1;
+        float2 a = x0, b = make_float2(0.f, 0.f);
+        static_for<H>([&](auto jj) {
+            constexpr int j = decltype(jj)::value + 1;
+            constexpr float c = (float)ct_cos(ct_angle<R, j * k>());
+            constexpr float sn = (float)ct_sin(ct_angle<R, j * k>());
+            a.x = fmaf(c, t[j - 1].x, a.x);
+            a.y = fmaf(c, t[j - 1].y, a.y);
+            b.x = fmaf(sn, u[j - 1].x, b.x);
+            b.y = fmaf(sn, u[j - 1].y, b.y);
+        });
+        const float2 ib = INV ? mul_pi(b) : mul_mi(b);
+        v[k] = cadd(a, ib);
+        v[R - k] = csub(a, ib);
+    });
+    v[0] = sum;
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft(float2* v) {
     if constexpr (R == 2) dft2<INV>(v);
+    else if constexpr (R == 11 || R == 13) dft_odd<R, INV>(v);
     else if constexpr (R == 3) dft3<INV>(v);
     else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
     else if constexpr (R == 5) dft5<INV>(v);
@@ -236,6 +313,8 @@ __device__ float2* fft_run(float2* a, float2* b, const float2* tw, const PassCfg
             case 5: fft_stage<5, INV>(a, b, tw, c.L, p, W, c.Wp); break;
             case 3: fft_stage<3, INV>(a, b, tw, c.L, p, W, c.Wp); break;
             case 7: fft_stage<7, INV>(a, b, tw, c.L, p, W, c.Wp); break;
+            case 11: fft_stage<11, INV>(a, b, tw, c.L, p, W, c.Wp); break;
+            case 13: fft_stage<13, INV>(a, b, tw, c.L, p, W, c.Wp); break;
         }
         __syncthreads();
         float2* t = a;

@@ -42,34 +42,6 @@ __device__ __forceinline__ float2 tw_get(const float2* tw, int m) {
     return w;
 }
 
-// ---- compile-time twiddles -----------------------------------------------------------------
-// W_R^m = exp(-2 pi i m / R) evaluated while compiling: the angle is reduced to [-pi, pi] and
-// sine / cosine are summed from their Taylor series in double (terms to x^31, error far below
-// float rounding), then rounded once to float. Exact quarter turns become swaps.
-constexpr double kTwoPi = 6.283185307179586476925286766559;
-
-constexpr double ct_sin(double x) {
-    double term = x, sum = x;
-    for (int k = 1; k < 16; ++k) {
-        term *= -x * x / (double)((2 * k) * (2 * k + 1));
-        sum += term;
-    }
-    return sum;
-}
-constexpr double ct_cos(double x) {
-    double term = 1.0, sum = 1.0;
-    for (int k = 1; k < 16; ++k) {
-        term *= -x * x / (double)((2 * k - 1) * (2 * k));
-        sum += term;
-    }
-    return sum;
-}
-template <int R, int M>
-constexpr double ct_angle() {
-    constexpr int m = ((M % R) + R) % R;
-    return kTwoPi * (double)(2 * m > R ? m - R : m) / (double)R;  // in [-pi, pi]
-}
-
 // a * W_R^M (INV: conjugate twiddle)
 template <int R, int M, bool INV>
 __device__ __forceinline__ float2 cmul_tw(float2 a) {
@@ -87,16 +59,6 @@ __device__ __forceinline__ float2 cmul_tw(float2 a) {
         constexpr float sn = (float)(INV ? ct_sin(ct_angle<R, M>()) : -ct_sin(ct_angle<R, M>()));
         return make_float2(fmaf(a.x, c, -a.y * sn), fmaf(a.x, sn, a.y * c));
     }
-}
-
-// Calls f(std::integral_constant<int, I>) for I = 0 .. N-1 (indices usable as constants).
-template <class F, int... I>
-__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
-    (f(std::integral_constant<int, I>{}), ...);
-}
-template <int N, class F>
-__device__ __forceinline__ void static_for(F&& f) {
-    static_for_impl(f, std::make_integer_sequence<int, N>{});
 }
 
 // In-register DFT of size R (composite sizes split as A x B with constant twiddles).

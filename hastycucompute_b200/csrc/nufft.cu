@@ -228,6 +228,22 @@ __global__ void k_tile_extra_fill(const int* extra_cnt, const int* extra_off, in
     for (int c = 0; c < n; ++c) extra[off + c] = make_int2((int)tile, c + 1);
 }
 
+// Tiles with more candidates than a subproblem holds, listed by the cluster size that spreads
+// them: K = 2, 4 or 8 CTAs (list k holds the tiles of K = 2 << k). List order is arbitrary; each
+// tile's result does not depend on it.
+__global__ void k_tile_classify(const int* bin_start, TileNbr t, int64_t ntiles, int maxp, int* cnt, int* lists) {
+    const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= ntiles) return;
+    const int tx = (int)(tile % t.nb[2]), ty = (int)((tile / t.nb[2]) % t.nb[1]), tz = (int)(tile / ((int64_t)t.nb[2] * t.nb[1]));
+    int64_t total = 0;
+    for_each_nbr_bin(t.nb, tz, ty, tx, [&](int bin) { total += bin_start[bin + 1] - bin_start[bin]; });
+    if (total <= maxp) return;
+    const int64_t nsub = (total + maxp - 1) / maxp;
+    const int k = nsub <= 2 ? 0 : (nsub <= 4 ? 1 : 2);
+    const int pos = atomicAdd(&cnt[k], 1);
+    lists[(int64_t)k * ntiles + pos] = (int)tile;
+}
+
 // ---------------------------------------------------------------------------------------------
 // execute kernels
 
@@ -251,22 +267,8 @@ __global__ void k_interleave_in(const float2* __restrict__ in, float2* __restric
     }
 }
 
-struct GridArgs {
-    GridGeom g;
-    const float* su[3];
-    const int* perm;
-    const int* bin_start;
-    const float2* inT;  // spread input [M][C], transforms interleaved, caller's point order
-    float2* grid;       // [nf0][nf1][nf2][C]
-    float2* out;        // interp output [C][M]
-    const int2* extra;
-    int maxp;
-    KbPoly kb;
-};
-
 constexpr int kGridThreads = 256;
 constexpr int kGridWarps = kGridThreads / 32;
-constexpr int kCoefFloats = kMaxWidth * (kMaxDeg + 1);
 constexpr int kSlotFloats = 3 * kMaxWidth;
 
 // Per point: fine coordinate -> first cell (wrapped) and the tap weights of each axis. The
@@ -1118,6 +1120,15 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
         p->wb[1] = 4;
         p->wb[2] = 8;
     }
+    // lanes-on-transforms spreading: 8^3 (3-D) or 16x32 (2-D) tiles, widths 4..8, more than four
+    // transforms, and at least two tiles along every non-unit axis (so no footprint wraps onto its
+    // own tile)
+    {
+        bool ok = (dim == 3 || dim == 2) && w >= 4 && w <= 8 && ntransf >= 5;
+        for (int ax = 3 - dim; ax < 3; ++ax) ok = ok && g.nb[ax] >= 2;
+        p->lc = p->lc_ok = ok;
+        p->lc_cc = ntransf >= 17 ? 32 : (ntransf >= 9 ? 16 : 8);
+    }
     p->beta = kb_beta(w, p->sigma);
     const double fit_err = kb_fit(&p->kb, w, p->beta);
     if (!(fit_err < 1e-6)) {
@@ -1255,7 +1266,31 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
         // unit axes: sorted coordinate arrays hold zeros
         for (int ax = 0; ax < 3; ++ax)
             if (!ca[ax] && p->su[ax] && M > 0) cudaMemsetAsync(p->su[ax], 0, sizeof(float) * M, s);
-        if (p->type == 1) {
+        if (p->type == 1 && p->lc) {
+            if (p->maxp_auto) p->maxp = auto_subproblem(M, g);
+            if (p->dense_list == nullptr) {
+                if ((st = dev_alloc(p, (void**)&p->dense_list, sizeof(int) * 3 * std::max<int64_t>(p->nbins, 1),
+                                    "dense tile lists")) != HB_OK)
+                    break;
+                if ((st = dev_alloc(p, (void**)&p->d_dense_cnt, sizeof(int) * 4, "dense tile counts")) != HB_OK) break;
+            }
+            TileNbr tn;
+            for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
+            if ((e = cudaMemsetAsync(p->d_dense_cnt, 0, sizeof(int) * 4, s)) != cudaSuccess) {
+                set_error(std::string("setpts memset: ") + cudaGetErrorString(e));
+                st = HB_ERR_CUDA;
+                break;
+            }
+            k_tile_classify<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins, p->maxp,
+                                                                              p->d_dense_cnt, p->dense_list);
+            if ((st = check_launch("k_tile_classify")) != HB_OK) break;
+            if ((e = cudaMemcpyAsync(p->n_dense, p->d_dense_cnt, sizeof(int) * 3, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+                set_error(std::string("setpts copy: ") + cudaGetErrorString(e));
+                st = HB_ERR_CUDA;
+                break;
+            }
+            p->n_extra = 0;
+        } else if (p->type == 1) {
             if (p->maxp_auto) p->maxp = auto_subproblem(M, g);
             TileNbr tn;
             for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
@@ -1453,7 +1488,10 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
             HB_TRY(check_launch("k_interleave_in"));
         }
         GridArgs a = grid_args(p);
-        HB_TRY(dispatch_cc(spread_cc(g), p, a, s, true));
+        if (p->lc)
+            HB_TRY(p->lc_cc == 8 ? spread_lc_cc8(p, a, s) : (p->lc_cc == 16 ? spread_lc_cc16(p, a, s) : spread_lc_cc32(p, a, s)));
+        else
+            HB_TRY(dispatch_cc(spread_cc(g), p, a, s, true));
         float2* cur = p->X;
         float2* other = p->Y;
         // axis 0: [nf0][nf1*nf2*C] -> [Nm0][...]
@@ -1534,6 +1572,17 @@ int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx) {
     return HB_OK;
 }
 
+int plan_set_spread_kernel(NufftPlan* p, int kind) {
+    HB_REQUIRE(!p->pts_set, HB_ERR_STATE, "set the spreading kernel before setpts");
+    HB_REQUIRE(kind == HB_SPREAD_AUTO || kind == HB_SPREAD_CELLS || kind == HB_SPREAD_TRANSFORMS, HB_ERR_INVALID_ARG,
+               "spreading kernel must be HB_SPREAD_AUTO, HB_SPREAD_CELLS or HB_SPREAD_TRANSFORMS");
+    HB_REQUIRE(kind != HB_SPREAD_TRANSFORMS || p->lc_ok, HB_ERR_INVALID_ARG,
+               "this plan cannot spread with the transforms on the lanes (needs 8^3 / 16x32 tiles, width 4..8, "
+               ">= 5 transforms, >= 2 tiles per axis)");
+    p->lc = kind == HB_SPREAD_CELLS ? false : p->lc_ok;
+    return HB_OK;
+}
+
 int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s) {
     HB_REQUIRE(p->type == 2, HB_ERR_INVALID_ARG, "coordinate gradient needs a type-2 plan");
     HB_REQUIRE(p->pts_set, HB_ERR_STATE, "coordinate gradient called before setpts");
@@ -1573,7 +1622,8 @@ void plan_free(NufftPlan* p) {
         if (p->tmp_u[ax]) cudaFree(p->tmp_u[ax]);
         p->tmp_u[ax] = nullptr;
     }
-    for (int** q : {&p->tmp_binid, &p->tmp_rank, &p->tmp_count, &p->tmp_ecnt, &p->tmp_eoff, &p->tmp_sums}) {
+    for (int** q : {&p->tmp_binid, &p->tmp_rank, &p->tmp_count, &p->tmp_ecnt, &p->tmp_eoff, &p->tmp_sums,
+                    &p->dense_list, &p->d_dense_cnt}) {
         if (*q) cudaFree(*q);
         *q = nullptr;
     }

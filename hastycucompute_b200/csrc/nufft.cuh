@@ -69,9 +69,40 @@ struct NufftPlan {
     int maxp = 4096;
     bool maxp_auto = true;
     int wb[3] = {2, 4, 4};
+    // lanes-on-transforms spreading (k_spread_lc): usable for this plan's shape (lc_ok), chosen
+    // (lc), its transform chunk, and the dense tiles of the current points grouped by cluster
+    // size K = 2, 4, 8
+    bool lc = false;
+    bool lc_ok = false;
+    int lc_cc = 0;
+    int* dense_list = nullptr;   // [3][nbins]
+    int* d_dense_cnt = nullptr;  // [4]
+    int n_dense[3] = {0, 0, 0};
     size_t device_bytes = 0;
 };
 
+
+// Arguments of the gridding kernels (spreading and interpolation).
+struct GridArgs {
+    GridGeom g;
+    const float* su[3];
+    const int* perm;
+    const int* bin_start;
+    const float2* inT;  // spread input [M][C], transforms interleaved, caller's point order
+    float2* grid;       // [nf0][nf1][nf2][C]
+    float2* out;        // interp output [C][M]
+    const int2* extra;
+    int maxp;
+    KbPoly kb;
+};
+
+constexpr int kCoefFloats = kMaxWidth * (kMaxDeg + 1);
+
+// Type-1 spreading with the transforms on the lanes (spread_lc.cuh; instances in
+// spread_lc{8,16,32}.cu) for plans with p->lc set, by transform chunk.
+int spread_lc_cc8(const NufftPlan* p, const GridArgs& a, cudaStream_t s);
+int spread_lc_cc16(const NufftPlan* p, const GridArgs& a, cudaStream_t s);
+int spread_lc_cc32(const NufftPlan* p, const GridArgs& a, cudaStream_t s);
 
 int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, int ntransf, float tol,
               int width, double upsampfac, int method);
@@ -79,6 +110,7 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
 int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s);
 int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s);
 int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx);
+int plan_set_spread_kernel(NufftPlan* p, int kind);
 void plan_free(NufftPlan* p);
 
 // Pieces reused by the Toeplitz kernel builder.

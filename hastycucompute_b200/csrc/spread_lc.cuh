@@ -1,0 +1,401 @@
+// Type-1 spreading with the transforms on the lanes.
+//
+// One CTA owns one tile of the fine grid (8x8x8 in 3-D, 16x32 in 2-D) for CC transforms. The 32
+// lanes of a warp are G = 32/CC groups of CC transforms; every thread keeps 4 rows x 8 cells of
+// its tile in registers for its one transform (64 accumulators): rows (2 z x 2 y) in 3-D, 4 y
+// in 2-D, 8 consecutive x cells per row. A warp's block is 1 x-segment of 8 cells x 4 rows per
+// group (groups take consecutive y rows).
+//
+// Candidate points (the tile's bin and its lower neighbours) pass through shared memory in
+// double-buffered chunks: per point the CC values (cp.async), the tile-relative z and y weights
+// (zero outside the footprint, so a row outside it multiplies by 0 and no row needs a branch)
+// and the raw x taps. A warp visits only the points whose footprint meets its block (one ballot
+// per 32 candidates). For a visited point every lane forms its 4 row products u_r = w_z w_y v and
+// adds w_x[x - x0] u_r to exactly the cells the footprint covers along x: the point's x offset is
+// the same for the whole warp, so a switch over it selects code whose cell range and tap indices
+// are compile-time constants.
+//
+// Dense tiles (more candidates than a subproblem holds) run as a thread-block cluster of K = 2, 4
+// or 8 CTAs: each CTA spreads 1/K of the candidates into registers, the partial tiles meet in
+// shared memory, and each CTA sums one K-th of the cells over the cluster's CTAs through
+// distributed shared memory in rank order before storing. No global atomics anywhere; every cell
+// is written exactly once and the sum order is fixed.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "fft2.cuh"
+#include "nufft.cuh"
+#include "timing.cuh"
+
+namespace hb {
+
+constexpr int kLcChunk = 128;  // candidates staged per chunk
+constexpr int kLcRec = 32;     // weight floats per staged point: wz_t[8] | wy_t[16] | wx[8]
+
+template <int CC, bool D3>
+struct LcShape {
+    static constexpr int G = 32 / CC;  // lane groups per warp
+    static constexpr int RZ = D3 ? 2 : 1;
+    static constexpr int RY = D3 ? 2 : 4;
+    static constexpr int T0 = D3 ? 8 : 1, T1 = D3 ? 8 : 16, T2 = D3 ? 8 : 32;
+    static constexpr int NZB = T0 / RZ, NYB = T1 / (G * RY), NXS = T2 / 8;
+    static constexpr int WARPS = NZB * NYB * NXS;
+    static constexpr int THREADS = WARPS * 32;
+    static constexpr int CELLS = T0 * T1 * T2;
+    // staging buffer: values float2[chunk][CC] | weights float[chunk][kLcRec] | packed first cells
+    static constexpr int kValF = kLcChunk * CC * 2;
+    static constexpr int kBufF = kValF + kLcChunk * kLcRec + kLcChunk;
+    static constexpr int kPartF = CELLS * CC * 2;  // one partial tile (cluster reduction)
+    static size_t smem_bytes(bool cluster) {
+        const int region = cluster ? (2 * kBufF > kPartF ? 2 * kBufF : kPartF) : 2 * kBufF;
+        return sizeof(float) * (size_t)(kCoefFloats + region);
+    }
+};
+static_assert(LcShape<32, true>::THREADS == 512 && LcShape<8, true>::THREADS == 128, "tile shape");
+static_assert(LcShape<32, false>::THREADS == 512 && LcShape<8, false>::THREADS == 128, "tile shape");
+
+// acc[r][x] += wx[x - RX] * u_r over the cells x in [0, 8) that the footprint [RX, RX + W) covers
+template <int W, int RX>
+__device__ __forceinline__ void lc_rows(float (&ar)[4][8], float (&ai)[4][8], const float (&wx)[8], const float (&ur)[4],
+                                        const float (&ui)[4]) {
+    constexpr int lo = RX < 0 ? 0 : RX;
+    constexpr int hi = (RX + W - 1) > 7 ? 7 : (RX + W - 1);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+#pragma unroll
+        for (int x = lo; x <= hi; ++x) {
+            ar[r][x] = fmaf(wx[x - RX], ur[r], ar[r][x]);
+            ai[r][x] = fmaf(wx[x - RX], ui[r], ai[r][x]);
+        }
+    }
+}
+
+#define HB_LC_CASE(K)                                                                 \
+    case K:                                                                           \
+        if constexpr ((K) < 8 + W - 1) lc_rows<W, (K) - (W - 1)>(ar, ai, wx, ur, ui); \
+        break;
+
+template <int W>
+__device__ __forceinline__ void lc_dispatch(int k, float (&ar)[4][8], float (&ai)[4][8], const float (&wx)[8],
+                                            const float (&ur)[4], const float (&ui)[4]) {
+    static_assert(W >= 2 && W <= 8, "lanes-on-transforms spreading takes widths 2..8");
+    switch (k) {
+        HB_LC_CASE(0) HB_LC_CASE(1) HB_LC_CASE(2) HB_LC_CASE(3) HB_LC_CASE(4)
+        HB_LC_CASE(5) HB_LC_CASE(6) HB_LC_CASE(7) HB_LC_CASE(8) HB_LC_CASE(9)
+        HB_LC_CASE(10) HB_LC_CASE(11) HB_LC_CASE(12) HB_LC_CASE(13) HB_LC_CASE(14)
+        default: break;
+    }
+}
+#undef HB_LC_CASE
+
+// tile_list == nullptr: one CTA per tile (blockIdx.x); tiles with more than maxp candidates are
+// left to the cluster launches. Otherwise CTA blockIdx.x spreads part blockIdx.x % K of tile
+// tile_list[blockIdx.x / K] inside a cluster of K CTAs.
+template <int CC, int W, bool D3>
+__global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
+    k_spread_lc(const GridArgs a, const int* __restrict__ tile_list, int K) {
+    using S = LcShape<CC, D3>;
+    extern __shared__ float4 sm_f4[];
+    float* coef = reinterpret_cast<float*>(sm_f4);
+    float* region = coef + kCoefFloats;
+    __shared__ int s_start[8], s_pref[9], s_nbin;
+    const GridGeom& g = a.g;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int grp = lane / CC, coil = lane % CC;
+
+    const int tile = tile_list ? tile_list[blockIdx.x / K] : (int)blockIdx.x;
+    const int part = tile_list ? (int)(blockIdx.x % K) : 0;
+    const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
+    const int org0 = tz * S::T0, org1 = ty * S::T1, org2 = tx * S::T2;
+    const int nf1 = g.nf[1], nf2 = g.nf[2];
+
+    // this warp's block and this group's rows
+    const int xs = warp % S::NXS, yb = (warp / S::NXS) % S::NYB, zb = warp / (S::NXS * S::NYB);
+    const int x0 = xs * 8, z0 = zb * S::RZ, y0w = yb * S::G * S::RY;
+    const int y0g = y0w + grp * S::RY;
+    constexpr int WZ = D3 ? W : 1;
+
+    for (int i = tid; i < kCoefFloats; i += S::THREADS) coef[i] = (&a.kb.coef[0][0])[i];
+    if (warp == 0) {
+        const int nz = g.nb[0] > 1 ? 2 : 1, ny = g.nb[1] > 1 ? 2 : 1, nx = g.nb[2] > 1 ? 2 : 1;
+        const int nbn = nz * ny * nx;
+        int st = 0, cnt = 0;
+        if (lane < nbn) {
+            const int dx = lane % nx, dy = (lane / nx) % ny, dz = lane / (nx * ny);
+            const int bz = (tz - dz + g.nb[0]) % g.nb[0], by = (ty - dy + g.nb[1]) % g.nb[1];
+            const int bx = (tx - dx + g.nb[2]) % g.nb[2];
+            const int bin = (bz * g.nb[1] + by) * g.nb[2] + bx;
+            st = a.bin_start[bin];
+            cnt = a.bin_start[bin + 1] - st;
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < nbn) {
+            s_start[lane] = st;
+            s_pref[lane] = incl - cnt;
+        }
+        if (lane == nbn - 1) {
+            s_pref[nbn] = incl;
+            s_nbin = nbn;
+        }
+    }
+    __syncthreads();
+    const int nbin = s_nbin;
+    const int total = s_pref[nbin];
+    if (!tile_list) {
+        if (total > a.maxp) return;  // a cluster launch spreads this tile
+        if (total == 0) {
+            // no point reaches the tile: 16-byte zero stores (a tile row of T2 cells x C values is
+            // contiguous and 16-byte aligned: T2 and the tile origin are multiples of 8)
+            const int rowf4 = (S::T2 * g.C) >> 1;
+            const int nrow = S::T0 * S::T1;
+            for (int i = tid; i < nrow * rowf4; i += S::THREADS) {
+                const int r = i / rowf4, c4 = i - r * rowf4;
+                const int zz = r / S::T1, yy = r - zz * S::T1;
+                float4* dst = reinterpret_cast<float4*>(
+                    a.grid + (((int64_t)(org0 + zz) * nf1 + (org1 + yy)) * nf2 + org2) * g.C);
+                dst[c4] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            return;
+        }
+    }
+    const int k_begin = (int)((int64_t)part * total / K);
+    const int k_end = (int)((int64_t)(part + 1) * total / K);
+    const float hw = a.kb.hw;
+    const bool vec = (g.C % 2) == 0;
+
+    // candidates visited interleaved across the tile's bins (8 segments, k -> segment k % 8)
+    const int seg_len = total >> 3, seg_rem = total & 7;
+    auto sorted_index = [&](int k0) -> int {
+        const int sgm = k0 & 7;
+        const int k = sgm * seg_len + min(sgm, seg_rem) + (k0 >> 3);
+        int b = 0;
+#pragma unroll
+        for (int j = 1; j < 8; ++j) b += (j < nbin && s_pref[j] <= k) ? 1 : 0;
+        return s_start[b] + (k - s_pref[b]);
+    };
+
+    auto stage = [&](int base, int cc0, float* buf) {
+        const int n = min(kLcChunk, k_end - base);
+        float2* bval = reinterpret_cast<float2*>(buf);
+        float* bwt = buf + S::kValF;
+        unsigned char* brel = reinterpret_cast<unsigned char*>(bwt + kLcChunk * kLcRec);
+        constexpr int CP = CC / 2;
+        for (int i = tid; i < n * CP; i += S::THREADS) {
+            const int q = i / CP, c = 2 * (i % CP);
+            float2* dst = bval + q * CC + c;
+            const int cg = cc0 + c;
+            const float2* src = a.inT + (int64_t)a.perm[sorted_index(base + q)] * g.C + cg;
+            if (vec && cg < g.C) {
+                cp_async16(dst, src);
+            } else {
+                if (cg < g.C) cp_async8(dst, src); else dst[0] = make_float2(0.f, 0.f);
+                if (cg + 1 < g.C) cp_async8(dst + 1, src + 1); else dst[1] = make_float2(0.f, 0.f);
+            }
+        }
+        for (int i = tid; i < 3 * n; i += S::THREADS) {
+            const int q = i / 3, ax = i - 3 * q;
+            float* rec = bwt + q * kLcRec;
+            int rel = 0;
+            if (ax == 0 && !D3) {
+                rec[0] = 1.f;
+#pragma unroll
+                for (int d = 1; d < 8; ++d) rec[d] = 0.f;
+            } else {
+                const float u = a.su[ax][sorted_index(base + q)];
+                const float v = __fsub_rn(u, hw);
+                const int ic = (int)ceilf(v);
+                const float sarg = fmaf(2.f, __fsub_rn((float)ic, v), -1.f);
+                const int nf = g.nf[ax];
+                const int T = ax == 0 ? S::T0 : (ax == 1 ? S::T1 : S::T2);
+                int iw = ic;
+                if (iw < 0) iw += nf;
+                if (iw >= nf) iw -= nf;
+                rel = iw - (ax == 0 ? org0 : (ax == 1 ? org1 : org2));
+                if (rel < 0) rel += nf;
+                if (rel >= T) rel -= nf;  // a footprint reaching the tile from below starts at -(W-1) .. -1
+                float t[W];
+#pragma unroll
+                for (int d = 0; d < W; ++d) t[d] = kb_tap(coef, a.kb.deg, d, sarg);
+                if (ax == 2) {
+#pragma unroll
+                    for (int d = 0; d < 8; ++d) rec[24 + d] = d < W ? t[d] : 0.f;
+                } else {
+                    float* wt = rec + (ax == 0 ? 0 : 8);
+                    for (int c = 0; c < T; ++c) wt[c] = 0.f;
+#pragma unroll
+                    for (int d = 0; d < W; ++d) {
+                        const int c = rel + d;
+                        if (c >= 0 && c < T) wt[c] = t[d];
+                    }
+                }
+            }
+            brel[q * 4 + ax] = (unsigned char)max(min(rel + 16, 255), 0);
+        }
+    };
+
+    for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
+        float ar[4][8], ai[4][8];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int x = 0; x < 8; ++x) ar[r][x] = ai[r][x] = 0.f;
+        const int nch = (k_end - k_begin + kLcChunk - 1) / kLcChunk;
+        if (nch > 0) stage(k_begin, cc0, region);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        for (int it = 0; it < nch; ++it) {
+            const int base = k_begin + it * kLcChunk;
+            if (it + 1 < nch) stage(base + kLcChunk, cc0, region + ((it + 1) & 1) * S::kBufF);
+            cp_async_commit();
+            {
+                const int n = min(kLcChunk, k_end - base);
+                const float* buf = region + (it & 1) * S::kBufF;
+                const float2* bval = reinterpret_cast<const float2*>(buf);
+                const float* bwt = buf + S::kValF;
+                const int* brel = reinterpret_cast<const int*>(bwt + kLcChunk * kLcRec);
+                for (int q0 = 0; q0 < n; q0 += 32) {
+                    const int qq = q0 + lane;
+                    bool hit = false;
+                    if (qq < n) {
+                        const int pk = brel[qq];
+                        const int rz = (pk & 0xff) - 16, ry = ((pk >> 8) & 0xff) - 16, rx = ((pk >> 16) & 0xff) - 16;
+                        hit = rz <= z0 + S::RZ - 1 && rz + WZ - 1 >= z0 && ry <= y0w + S::G * S::RY - 1 &&
+                              ry + W - 1 >= y0w && rx <= x0 + 7 && rx + W - 1 >= x0;
+                    }
+                    unsigned bits = __ballot_sync(0xffffffffu, hit);
+                    while (bits) {
+                        const int q = q0 + __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        const int k = ((brel[q] >> 16) & 0xff) - 16 - x0 + (W - 1);
+                        const float2 v = bval[q * CC + coil];
+                        const float* rec = bwt + q * kLcRec;
+                        float rw[4];
+                        if constexpr (D3) {
+                            const float2 wz2 = *reinterpret_cast<const float2*>(rec + z0);
+                            const float2 wy2 = *reinterpret_cast<const float2*>(rec + 8 + y0g);
+                            rw[0] = wz2.x * wy2.x;
+                            rw[1] = wz2.x * wy2.y;
+                            rw[2] = wz2.y * wy2.x;
+                            rw[3] = wz2.y * wy2.y;
+                        } else {
+                            const float4 wy4 = *reinterpret_cast<const float4*>(rec + 8 + y0g);
+                            rw[0] = wy4.x;
+                            rw[1] = wy4.y;
+                            rw[2] = wy4.z;
+                            rw[3] = wy4.w;
+                        }
+                        float ur[4], ui[4];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            ur[r] = rw[r] * v.x;
+                            ui[r] = rw[r] * v.y;
+                        }
+                        const float4 xa = *reinterpret_cast<const float4*>(rec + 24);
+                        const float4 xb = *reinterpret_cast<const float4*>(rec + 28);
+                        const float wx[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+                        lc_dispatch<W>(k, ar, ai, wx, ur, ui);
+                    }
+                }
+            }
+            cp_async_wait_all();
+            __syncthreads();
+        }
+        const bool coil_ok = cc0 + coil < g.C;
+        if (K == 1) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int z = z0 + (D3 ? (r >> 1) : 0), y = y0g + (D3 ? (r & 1) : r);
+                float2* row = a.grid + (((int64_t)(org0 + z) * nf1 + (org1 + y)) * nf2 + org2 + x0) * g.C + cc0 + coil;
+                if (coil_ok) {
+#pragma unroll
+                    for (int x = 0; x < 8; ++x) row[(int64_t)x * g.C] = make_float2(ar[r][x], ai[r][x]);
+                }
+            }
+        } else {
+            // partial tiles meet in shared memory; CTA `part` sums cells [part, part+1) * CELLS / K
+            namespace cgx = cooperative_groups;
+            cgx::cluster_group cluster = cgx::this_cluster();
+            float2* ptile = reinterpret_cast<float2*>(region);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int z = z0 + (D3 ? (r >> 1) : 0), y = y0g + (D3 ? (r & 1) : r);
+#pragma unroll
+                for (int x = 0; x < 8; ++x)
+                    ptile[((z * S::T1 + y) * S::T2 + x0 + x) * CC + coil] = make_float2(ar[r][x], ai[r][x]);
+            }
+            cluster.sync();
+            const int per = S::CELLS * CC / K;
+            for (int i = part * per + tid; i < (part + 1) * per; i += S::THREADS) {
+                float2 sum = make_float2(0.f, 0.f);
+                for (int k2 = 0; k2 < K; ++k2) {
+                    const float2* rt = cluster.map_shared_rank(ptile, k2);
+                    const float2 v = rt[i];
+                    sum.x += v.x;
+                    sum.y += v.y;
+                }
+                const int c = i % CC, cell = i / CC;
+                if (cc0 + c < g.C) {
+                    const int x = cell % S::T2, y = (cell / S::T2) % S::T1, z = cell / (S::T2 * S::T1);
+                    a.grid[(((int64_t)(org0 + z) * nf1 + (org1 + y)) * nf2 + org2 + x) * g.C + cc0 + c] = sum;
+                }
+            }
+            cluster.sync();  // the partial tiles stay readable until every CTA has summed its share
+        }
+    }
+}
+
+// Host launch: one CTA per tile for the tiles within one subproblem, then one cluster launch per
+// cluster size for the dense tiles.
+template <int CC, int W, bool D3>
+inline int launch_spread_lc(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
+    using S = LcShape<CC, D3>;
+    auto kern = k_spread_lc<CC, W, D3>;
+    const size_t sm_plain = S::smem_bytes(false), sm_cluster = S::smem_bytes(true);
+    HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(sm_plain, sm_cluster)));
+    {
+        TimedSection ts("spread", s);
+        kern<<<(unsigned)p->nbins, S::THREADS, sm_plain, s>>>(a, nullptr, 1);
+        HB_TRY(check_launch("k_spread_lc"));
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (p->n_dense[k] == 0) continue;
+        const int K = 2 << k;
+        TimedSection ts("spread_dense", s);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(K * p->n_dense[k]), 1, 1);
+        cfg.blockDim = dim3(S::THREADS, 1, 1);
+        cfg.dynamicSmemBytes = sm_cluster;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)K;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        HB_CUDA(cudaLaunchKernelEx(&cfg, kern, a, (const int*)(p->dense_list + (int64_t)k * p->nbins), K));
+    }
+    return HB_OK;
+}
+
+template <int CC, bool D3>
+inline int launch_spread_lc_w(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
+    switch (p->g.wa[2]) {
+        case 4: return launch_spread_lc<CC, 4, D3>(p, a, s);
+        case 5: return launch_spread_lc<CC, 5, D3>(p, a, s);
+        case 6: return launch_spread_lc<CC, 6, D3>(p, a, s);
+        case 7: return launch_spread_lc<CC, 7, D3>(p, a, s);
+        default: return launch_spread_lc<CC, 8, D3>(p, a, s);
+    }
+}
+
+}  // namespace hb

@@ -1,0 +1,11 @@
+// Instances of the lanes-on-transforms spreading kernel for 32 transforms per lane group (one
+// compilation unit per transform chunk so they build in parallel).
+#include "spread_lc.cuh"
+
+namespace hb {
+
+int spread_lc_cc32(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
+    return p->g.dim == 3 ? launch_spread_lc_w<32, true>(p, a, s) : launch_spread_lc_w<32, false>(p, a, s);
+}
+
+}  // namespace hb

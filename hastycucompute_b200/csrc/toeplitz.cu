@@ -52,9 +52,9 @@ static int toep_geom(ToepGeom* t, int dim, const int64_t* shape, int64_t B) {
     }
     for (int ax = 3 - dim; ax < 3; ++ax) {
         int r = t->L[ax];
-        for (int p : {2, 3, 5, 7})
+        for (int p : {2, 3, 5, 7, 11, 13})
             while (r % p == 0) r /= p;
-        HB_REQUIRE(r == 1, HB_ERR_INVALID_ARG, "2N must be 2,3,5,7-smooth on every axis");
+        HB_REQUIRE(r == 1, HB_ERR_INVALID_ARG, "2N must have no prime factor above 13 on any axis");
     }
     return HB_OK;
 }
@@ -800,14 +800,14 @@ static int noalloc_len(int L, float2* tw, cudaStream_t s, FftLen* f) {
     f->nrad = 0;
     f->tw = tw;
     int rest = L;
-    for (int r : {8, 4, 2, 5, 3, 7}) {
+    for (int r : {8, 4, 2, 5, 3, 7, 11, 13}) {
         while (rest % r == 0 && rest > 1) {
             HB_REQUIRE(f->nrad < kMaxRadices, HB_ERR_INVALID_ARG, "FFT length has too many factors");
             f->rad[f->nrad++] = r;
             rest /= r;
         }
     }
-    HB_REQUIRE(rest == 1, HB_ERR_INVALID_ARG, "2N must be 2,3,5,7-smooth on every axis");
+    HB_REQUIRE(rest == 1, HB_ERR_INVALID_ARG, "2N must have no prime factor above 13 on any axis");
     k_fill_twiddles<<<(unsigned)ceil_div(L, 256), 256, 0, s>>>(tw, L);
     return check_launch("k_fill_twiddles");
 }

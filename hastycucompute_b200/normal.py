@@ -71,7 +71,7 @@ class SenseOp:
     """Plain SENSE A (forward) / A^H (adjoint) with batched coils on one NUFFT plan pair."""
 
     def __init__(self, coords: Sequence[torch.Tensor], smaps: torch.Tensor, kernel_width: int = 0, tol: float = 1e-5,
-                 scale: float = 1.0):
+                 scale: float = 1.0, spread_tuning: Optional[dict] = None):
         self.smaps = smaps.contiguous()
         self.shape = tuple(smaps.shape[1:])
         self.ncoils = smaps.shape[0]
@@ -79,6 +79,9 @@ class SenseOp:
         opts = NufftOpts(nmodes=self.shape, ntransf=self.ncoils, tol=tol, kernel_width=kernel_width)
         self.fwd = NufftPlan(NufftType.TYPE_2, opts)
         self.adj = NufftPlan(NufftType.TYPE_1, opts)
+        if spread_tuning is not None:  # an autotune.tune_spread choice for the adjoint's spreading
+            from .autotune import apply
+            apply(self.adj, spread_tuning)
         self.setpts(coords)
 
     def setpts(self, coords: Sequence[torch.Tensor]) -> None:

@@ -104,6 +104,17 @@ int hb_nufft_execute(hb_nufft_plan plan, const void* in, void* out, void* stream
 int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block_z, int block_y,
                                int block_x);
 
+/* Spreading kernel of a type-1 plan, before its setpts (no counterpart in the reference, whose
+ * spreading method is cufinufft's GM / GM_SORT / SM choice, fft/nufft.cppm:119-139):
+ * HB_SPREAD_AUTO (transforms on the lanes when the plan allows it: 8^3 or 16x32 tiles, widths
+ * 4..8, 5 or more transforms, two or more tiles per axis), HB_SPREAD_CELLS (one cell per lane,
+ * any plan), HB_SPREAD_TRANSFORMS (transforms on the lanes; HB_ERR_INVALID_ARG where the plan
+ * does not allow it). Every choice computes the same sums. */
+#define HB_SPREAD_AUTO       0
+#define HB_SPREAD_CELLS      1
+#define HB_SPREAD_TRANSFORMS 2
+int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind);
+
 /* Coordinate gradient (no counterpart in the reference, which has no derivatives): with a
  * type-2 plan (sign s) whose points are set, writes to grad ([dim][M] float, image order)
  *   grad[i][j] = -(nf_i / 2 pi) Re( sum_c h[c][j] sum_l G_c[l] dPhi_i(l - u_j) )

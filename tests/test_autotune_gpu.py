@@ -1,4 +1,6 @@
-"""Spreading autotuner: every candidate gives the default's result; the choice is cached."""
+"""Spreading autotuner: every candidate (both kernels, every cell block, small and large
+subproblems) gives the oracle's result; the choice is cached; a plan that cannot put the
+transforms on the lanes refuses that kernel."""
 import numpy as np
 import pytest
 
@@ -18,12 +20,14 @@ def test_every_tuning_gives_the_same_transform(cuda, nmodes, w):
     c = crand(rng, T, M)
     ref = gridding.nufft1(coords, c, nmodes, w=w)
     blocks = autotune.BLOCKS_3D if len(nmodes) == 3 else autotune.BLOCKS_2D
-    for block in blocks:
-        for maxp in (64, 4096):
-            p = hb.NufftPlan(hb.NufftType.TYPE_1, hb.NufftOpts(nmodes=nmodes, ntransf=T, kernel_width=w))
-            p.set_spread_tuning(maxp, block)
-            p.setpts([to_dev(x, cuda) for x in coords])
-            assert relerr(to_np(p(to_dev(c, cuda))), ref) <= 1e-5, (block, maxp)
+    for kernel, bl in (("cells", blocks), ("transforms", blocks[:1])):
+        for block in bl:
+            for maxp in (64, 4096):
+                p = hb.NufftPlan(hb.NufftType.TYPE_1, hb.NufftOpts(nmodes=nmodes, ntransf=T, kernel_width=w))
+                p.set_spread_kernel(kernel)
+                p.set_spread_tuning(maxp, block)
+                p.setpts([to_dev(x, cuda) for x in coords])
+                assert relerr(to_np(p(to_dev(c, cuda))), ref) <= 1e-5, (kernel, block, maxp)
 
 
 @pytest.mark.gpu
@@ -33,9 +37,9 @@ def test_tuner_picks_and_caches(cuda, tmp_path, monkeypatch):
     monkeypatch.setenv("HASTY_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
     rng = np.random.default_rng(3)
     coords = [to_dev(x, cuda) for x in rand_coords(rng, 3, 30000)]
-    cand = [((2, 4, 4), 1024), ((4, 4, 2), 2048), ((1, 4, 8), 512)]
+    cand = [("cells", (2, 4, 4), 1024), ("cells", (4, 4, 2), 2048), ("transforms", (2, 4, 4), 512)]
     first = autotune.tune_spread((24, 24, 24), 8, coords, 6, candidates=cand)
-    assert not first["cached"] and (tuple(first["block"]), first["max_candidates"]) in cand
+    assert not first["cached"] and (first["kernel"], tuple(first["block"]), first["max_candidates"]) in cand
     assert len(first["timings"]) == 3
     again = autotune.tune_spread((24, 24, 24), 8, coords, 6, candidates=cand)
     assert again["cached"] and again["block"] == first["block"]
@@ -53,3 +57,12 @@ def test_tuning_arguments_are_checked_on_the_host():
     h = C.c_void_p()
     # makeplan allocates device memory, so only the pure argument checks run here
     assert lib.hb_nufft_set_spread_tuning(None, 1024, 2, 4, 4) == 1
+
+
+@pytest.mark.gpu
+def test_transforms_on_lanes_is_refused_where_the_plan_does_not_allow_it(cuda):
+    import hastycucompute_b200 as hb
+    p = hb.NufftPlan(hb.NufftType.TYPE_1, hb.NufftOpts(nmodes=(16, 16, 16), ntransf=2, kernel_width=6))
+    with pytest.raises(hb.HastyError, match="INVALID_ARG"):
+        p.set_spread_kernel("transforms")
+    p.set_spread_kernel("cells")

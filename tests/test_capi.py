@@ -105,7 +105,8 @@ def test_toeplitz_workspace_size_is_host_arithmetic():
     assert n.value == 8 * (N * N * 2 * N * B + N * 2 * N * 2 * N * B)
     assert lib.hb_toeplitz_workspace_size(2, _lib.i64_array([256, 256]), 12, C.byref(n)) == 0
     assert n.value == 8 * 256 * 512 * 12
-    assert lib.hb_toeplitz_workspace_size(3, _lib.i64_array([11, 8, 8]), 1, C.byref(n)) == 1  # 22 not 2,3,5,7-smooth
+    assert lib.hb_toeplitz_workspace_size(3, _lib.i64_array([11, 8, 8]), 1, C.byref(n)) == 0  # 22 = 2 * 11
+    assert lib.hb_toeplitz_workspace_size(3, _lib.i64_array([17, 8, 8]), 1, C.byref(n)) == 1  # 34 = 2 * 17
     assert lib.hb_toeplitz_workspace_size(1, _lib.i64_array([8]), 1, C.byref(n)) == 1
 
 

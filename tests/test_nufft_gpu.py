@@ -246,3 +246,25 @@ def test_register_fft_lengths(cuda, nmodes, w):
     p2 = _plan(hb, hb.NufftType.TYPE_2, nmodes, T, w)
     p2.setpts([to_dev(x, cuda) for x in coords])
     assert relerr(to_np(p2(to_dev(f, cuda))), gridding.nufft2(coords, f, w=w)) <= PARITY
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,nmodes,M,T,w", [(3, (24, 20, 16), 6000, 8, 6), (2, (40, 36), 4000, 12, 8),
+                                               (3, (32, 32, 32), 8000, 32, 7)])
+def test_upsampfac_1_25(cuda, dim, nmodes, M, T, w):
+    """nufft_upsamp_cuda UPSAMP_1_25 (cpp/corelib/lib/fft/nufft.cppm:59-63, 148-152): the fine grid
+    is 1.25 N (rounded up to the tile / FFT rule) and the Kaiser-Bessel shape follows sigma; both
+    types against the gridding oracle at the same sigma."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(M + T)
+    coords = rand_coords(rng, dim, M)
+    c = crand(rng, T, M)
+    f = crand(rng, T, *nmodes)
+    opts = hb.NufftOpts(nmodes=nmodes, ntransf=T, kernel_width=w, upsamp=hb.NufftUpsamp.UPSAMP_1_25)
+    p1 = hb.NufftPlan(hb.NufftType.TYPE_1, opts)
+    p1.setpts([to_dev(x, cuda) for x in coords])
+    assert p1.info().fine == kb.fine_grid(nmodes, w, 1.25)
+    assert relerr(to_np(p1(to_dev(c, cuda))), gridding.nufft1(coords, c, nmodes, w=w, sigma=1.25)) <= PARITY
+    p2 = hb.NufftPlan(hb.NufftType.TYPE_2, opts)
+    p2.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p2(to_dev(f, cuda))), gridding.nufft2(coords, f, w=w, sigma=1.25)) <= PARITY

@@ -39,7 +39,7 @@ FLAGS = [
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape", [(6, 8, 10), (16, 16, 16), (12, 10), (32, 30)])
+@pytest.mark.parametrize("shape", [(6, 8, 10), (16, 16, 16), (12, 10), (32, 30), (11, 13, 6), (22, 13)])
 @pytest.mark.parametrize("flags", FLAGS)
 @pytest.mark.parametrize("use_m2", [False, True])
 def test_multiplication_flags(cuda, shape, flags, use_m2):
@@ -84,22 +84,31 @@ def test_sense_normal(cuda, shape, C):
 
 
 @pytest.mark.gpu
-def test_sense_normal_is_scaled_AhA(cuda):
-    """T = (1/n) A^H diag(w) A: the fused normal op equals the plain SENSE pair up to NUFFT error."""
+def test_plain_sense_normal_matches_oracle_and_toeplitz(cuda):
+    """The plain SENSE normal operator S^H A^H A S (type 2 then type 1, as
+    hasty_python/right_precond_test.py:48-73 applies it) against the FP64 gridding oracle, and the
+    fused Toeplitz normal operator against the oracle's straight one built from the same points."""
     import hastycucompute_b200 as hb
     from hastycucompute_b200 import synthetic
+    from oracle import gridding
     rng = np.random.default_rng(2)
     shape, C, M, w = (16, 16, 16), 8, 12000, 6
     coords = rand_coords(rng, 3, M)
     S = synthetic.coil_maps(C, shape)
     x = crand(rng, *shape)
     dc = [to_dev(c, cuda) for c in coords]
+    sense = hb.SenseOp(dc, to_dev(S, cuda), kernel_width=w)
+    plain = to_np(sense.normal(to_dev(x, cuda)))
+    S128 = S.astype(np.complex128)
+    y = gridding.nufft2(coords, S128 * x[None], w=w)
+    ref_plain = np.sum(np.conj(S128) * gridding.nufft1(coords, y, shape, w=w), axis=0)
+    assert relerr(plain, ref_plain) <= PARITY
     K = hb.build_toeplitz_kernel(dc, shape, kernel_width=w)
     op = hb.NormalTT1Op(K, to_dev(S, cuda))
     got = to_np(op(to_dev(x, cuda)))
-    sense = hb.SenseOp(dc, to_dev(S, cuda), kernel_width=w)
-    plain = to_np(sense.normal(to_dev(x, cuda))) / np.prod(shape)
-    assert relerr(got, plain) <= 1e-4
+    assert relerr(got, otp.sense_normal(x, S, otp.toeplitz_kernel(coords, shape, w=w))) <= PARITY
+    # and T = (1/n) A^H A holds up to the NUFFT error of w = 6
+    assert relerr(got, plain / np.prod(shape)) <= 1e-4
 
 
 @pytest.mark.gpu
@@ -114,7 +123,8 @@ def test_workspace_argument(cuda):
     Kt = hb.transform_toeplitz_kernel(to_dev(K, cuda))
     ws = tp.make_workspace(shape, B, cuda)
     out = torch.zeros((B, *shape), dtype=torch.complex64, device=cuda)
-    hb.toeplitz_multiply(to_dev(inp, cuda), Kt, ws)
+    got = hb.toeplitz_multiply(to_dev(inp, cuda), Kt, ws)
+    assert relerr(to_np(got), otp.toeplitz_multiply(inp, K.astype(np.complex128))) <= PARITY
     small = torch.empty(10, dtype=torch.complex64, device=cuda)
     with pytest.raises(hb.HastyError, match="WORKSPACE"):
         hb.toeplitz_multiplication(to_dev(inp, cuda), out, Kt, small)
@@ -152,3 +162,18 @@ def test_toeplitz_kernel_register_lengths(cuda):
     K = hb.build_toeplitz_kernel([to_dev(c, cuda) for c in coords], shape, kernel_width=w)
     ref = otp.toeplitz_kernel(coords, shape, None, w=w)
     assert relerr(to_np(K), ref) <= PARITY
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,C", [((176, 176, 176), 2), ((176, 208, 220), 2), ((208, 220), 4), ((26, 22, 12), 5)])
+def test_sense_normal_lengths_with_factors_11_13(cuda, shape, C):
+    """2N with a prime factor 11 or 13 (352, 416, 440, 52, 44): the radix-11 / radix-13 Stockham
+    stages. The reference convolves any length through VkFFT (cpp/corelib/lib/fft/toeplitz.cppm:449-480)."""
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import synthetic
+    rng = np.random.default_rng(sum(shape))
+    x = crand(rng, *shape)
+    S = synthetic.coil_maps(C, shape)
+    K = crand(rng, *[2 * s for s in shape]).astype(np.complex128)
+    op = hb.NormalTT1Op(to_dev(K.astype(np.complex64), cuda), to_dev(S, cuda))
+    assert relerr(to_np(op(to_dev(x, cuda))), otp.sense_normal(x, S, K, fast=True)) <= PARITY
