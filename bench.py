@@ -387,7 +387,7 @@ def run_ours(args, wl_name: str):
 
     # ---- batched multi-frame recon vs per-frame plain-operator loop ----------------------------
     if not args.no_frames:
-        extra["frames"] = bench_frames(args, hb, dev, stream)
+        extra["frames"] = bench_frames(args, hb, dev, stream, world, rank)
         torch.cuda.empty_cache()
 
     # ---- configurations 0, 3 and 4 at their own sizes -------------------------------------------
@@ -480,46 +480,63 @@ def bench_nufft(args, hb, _lib, coords, wl, dev, stream, hbm_peak):
     return res
 
 
-def bench_frames(args, hb, dev, stream, nframes=24, shape=(128, 128, 128), C=16, iters=15, w=4):
+def bench_frames(args, hb, dev, stream, world=1, rank=0, nframes=24, shape=(128, 128, 128), C=16, iters=15, w=4):
     """Batched dynamic recon: frames with ragged golden-means radial trajectories (300-700 spokes x
-    128 samples), per-frame Toeplitz kernels, one batched graph-captured CG (all frames and coils
-    in one launch per pass) against a per-frame loop of CG on the plain NUFFT SENSE operator."""
+    128 samples), per-frame Toeplitz kernels, and three recons of the same right-hand sides:
+    - batched: one graph-captured CG over all frames (all frames and coils in one launch per pass);
+    - Toeplitz loop: a graph-captured CG on the single-frame fused operator, frame after frame;
+    - plain loop: CG on the plain NUFFT SENSE operator (type 2 then type 1 per apply), frame after
+      frame, with the adjoint's spreading autotuned for the problem.
+    With several ranks every rank reconstructs its share of the frames (split by sample count) and
+    the times are the slowest rank's."""
     import torch
-    from hastycucompute_b200 import synthetic
+    from hastycucompute_b200 import autotune, synthetic
+    from hastycucompute_b200.frames import frame_partition
     rng = np.random.default_rng(3)
     n = int(np.prod(shape))
     spokes = rng.integers(300, 701, nframes)
-    frames = [synthetic.golden_means_radial(int(ns), 128, offset=int(spokes[:f].sum())) for f, ns in enumerate(spokes)]
-    xs = synthetic.dynamic_images(nframes, shape)
+    ids = frame_partition(nframes, world, rank, [int(v) * 128 for v in spokes])
+    F = len(ids)
+    frames = [synthetic.golden_means_radial(int(spokes[f]), 128, offset=int(spokes[:f].sum())) for f in ids]
+    xs = synthetic.dynamic_images(nframes, shape)[ids[0]: ids[-1] + 1]
     S = torch.from_numpy(synthetic.coil_maps(C, shape)).to(dev)
-    t0 = time.perf_counter()
     dcoords = [[torch.from_numpy(np.ascontiguousarray(c)).to(dev) for c in fc] for fc in frames]
+    t0 = time.perf_counter()
     Ks = hb.build_toeplitz_kernels(dcoords, shape, kernel_width=w)
     torch.cuda.synchronize()
     t_kernels = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = autotune.tune_spread(shape, C, dcoords[0], w, reps=2, use_cache=True)
+    t_tune = time.perf_counter() - t0
     # data y_f = A_f (S x_f) + noise, right-hand sides b_f = (1/n) S^H A_f^H y_f (one plan pair,
     # re-pointed per frame)
-    b = torch.empty((nframes, *shape), dtype=torch.complex64, device=dev)
-    so = hb.SenseOp(dcoords[0], S, kernel_width=w, scale=1.0 / math.sqrt(n))
-    for f in range(nframes):
-        so.setpts(dcoords[f])
-        y = so.forward(torch.from_numpy(xs[f]).to(dev))
+    b = torch.empty((F, *shape), dtype=torch.complex64, device=dev)
+    so = hb.SenseOp(dcoords[0], S, kernel_width=w, scale=1.0 / math.sqrt(n), spread_tuning=tune)
+    for i, f in enumerate(ids):
+        so.setpts(dcoords[i])
+        y = so.forward(torch.from_numpy(xs[i]).to(dev))
         y = y + torch.from_numpy(synthetic.noise(tuple(y.shape), 1e-3 * float(y.abs().max()), seed=2 + f)).to(dev)
-        b[f] = so.adjoint(y)
-    op = hb.BatchedNormalOp(Ks, S)
-    solver = hb.BatchedCGSolver(lambda v, o: op.apply(v, o), nframes, shape, dev, max_iter=iters, tol=0.0, graph=True)
-    x0 = torch.zeros((nframes, *shape), dtype=torch.complex64, device=dev)
-    solver.solve(x0, b)  # capture + warm-up
-    torch.cuda.synchronize()
+        b[i] = so.adjoint(y)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    xb = solver.solve(x0, b)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_batched = e0.elapsed_time(e1) / 1e3
-    xb = xb.clone()
+
+    def timed_region(fn):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3, world, dev)
+
+    # batched
+    op = hb.BatchedNormalOp(Ks, S)
+    solver = hb.BatchedCGSolver(lambda v, o: op.apply(v, o), F, shape, dev, max_iter=iters, tol=0.0, graph=True)
+    x0 = torch.zeros((F, *shape), dtype=torch.complex64, device=dev)
+    solver.solve(x0, b)  # capture + warm-up
+    t_batched = timed_region(lambda: solver.solve(x0, b))
+    xb = solver.x.clone()
     acc = None
-    if not args.no_check:
+    if not args.no_check and rank == 0:
         # frame 0 of the batched recon against the FP64 oracle CG on its own straight operator
         from oracle import cg as ocg, toeplitz as otp
         Sn = S.cpu().numpy().astype(np.complex128)
@@ -529,30 +546,49 @@ def bench_frames(args, hb, dev, stream, nframes=24, shape=(128, 128, 128), C=16,
         acc = _rel(xb[0].cpu().numpy(), x_ref)
     del solver, op
     torch.cuda.empty_cache()
+    # per-frame loop of the fused single-frame operator: one operator and one captured CG whose
+    # kernel buffer takes each frame's transformed kernel in turn
+    kts = [hb.transform_toeplitz_kernel(Ks[i].contiguous()) for i in range(F)]
+    op1 = hb.NormalTT1Op(kts[0].clone(), S, transformed=True)
+    sv1 = hb.CGSolver(lambda v, o: op1.apply(v, o), shape, dev, max_iter=iters, tol=0.0, graph=True)
+    sv1.solve(x0[0], b[0])  # capture + warm-up
+    xt = torch.empty_like(xb)
+
+    def toeplitz_loop():
+        for i in range(F):
+            op1.kernel_t.copy_(kts[i])
+            xt[i] = sv1.solve(x0[i], b[i])
+
+    t_tloop = timed_region(toeplitz_loop)
+    del sv1, op1, kts
+    torch.cuda.empty_cache()
     # per-frame loop with the plain operator (NUFFT type 2 then type 1 per apply): the frame's
     # points are set, then CG runs on that frame
     sv = hb.CGSolver(lambda v, o: o.copy_(so.normal(v)), shape, dev, max_iter=iters, tol=0.0)
     so.setpts(dcoords[0])
     sv.solve(x0[0], b[0])  # warm-up
-    torch.cuda.synchronize()
     xl = torch.empty_like(xb)
-    t0 = time.perf_counter()
-    e0.record(stream)
-    for f in range(nframes):
-        so.setpts(dcoords[f])
-        xl[f] = sv.solve(x0[f], b[f])
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_loop = max(e0.elapsed_time(e1) / 1e3, 0.0)
+
+    def plain_loop():
+        for i in range(F):
+            so.setpts(dcoords[i])
+            xl[i] = sv.solve(x0[i], b[i])
+
+    t_loop = timed_region(plain_loop)
     diff = float(torch.linalg.vector_norm(xb - xl) / torch.linalg.vector_norm(xl))
+    tdiff = float(torch.linalg.vector_norm(xb - xt) / torch.linalg.vector_norm(xt))
     return {"workload": f"{nframes} frames x {shape[0]}^3, {C} coils, golden-means radial 300-700 spokes x 128, "
                         f"KB w={w}, {iters} CG iterations",
-            "samples_per_frame": [int(v) * 128 for v in spokes],
+            "samples_per_frame": [int(v) * 128 for v in spokes], "ranks": world,
             "batched_recons_per_s": round(nframes / t_batched, 3), "batched_s": round(t_batched, 3),
-            "looped_recons_per_s": round(nframes / t_loop, 3), "looped_s": round(t_loop, 3),
-            "speedup": round(t_loop / t_batched, 2), "batched_vs_looped_rel_diff": diff,
+            "toeplitz_looped_recons_per_s": round(nframes / t_tloop, 3), "toeplitz_looped_s": round(t_tloop, 3),
+            "plain_looped_recons_per_s": round(nframes / t_loop, 3), "plain_looped_s": round(t_loop, 3),
+            "batching_gain": round(t_tloop / t_batched, 3), "toeplitz_gain": round(t_loop / t_tloop, 3),
+            "speedup_vs_plain_loop": round(t_loop / t_batched, 2),
+            "batched_vs_toeplitz_looped_rel_diff": tdiff, "batched_vs_plain_looped_rel_diff": diff,
             "batched_frame0_rel_err_vs_fp64_oracle_cg": acc,
-            "toeplitz_kernels_s": round(t_kernels, 3), "graph_captured": True}
+            "spread_tuning": {k: tune[k] for k in ("kernel", "block", "max_candidates", "ms")},
+            "tuning_s": round(t_tune, 2), "toeplitz_kernels_s": round(t_kernels, 3), "graph_captured": True}
 
 
 def bench_configs(args, hb, dev, stream):
