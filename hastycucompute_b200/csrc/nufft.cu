@@ -228,20 +228,24 @@ __global__ void k_tile_extra_fill(const int* extra_cnt, const int* extra_off, in
     for (int c = 0; c < n; ++c) extra[off + c] = make_int2((int)tile, c + 1);
 }
 
-// Tiles with more candidates than a subproblem holds, listed by the cluster size that spreads
-// them: K = 2, 4 or 8 CTAs (list k holds the tiles of K = 2 << k). List order is arbitrary; each
-// tile's result does not depend on it.
-__global__ void k_tile_classify(const int* bin_start, TileNbr t, int64_t ntiles, int maxp, int* cnt, int* lists) {
+// Dense tiles (more candidates than a subproblem holds) for the lanes-on-transforms kernel: a
+// tile of `total` candidates is spread in nsub = ceil(total / maxp) parts, each into its own
+// scratch slot. cnt[tile] = nsub for dense tiles, 0 otherwise; the fill writes one work entry
+// {tile, part, nsub, first slot} per part at the scanned offsets (slots are numbered like entries).
+__global__ void k_tile_parts_count(const int* bin_start, TileNbr t, int64_t ntiles, int maxp, int* cnt) {
     const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tile >= ntiles) return;
     const int tx = (int)(tile % t.nb[2]), ty = (int)((tile / t.nb[2]) % t.nb[1]), tz = (int)(tile / ((int64_t)t.nb[2] * t.nb[1]));
     int64_t total = 0;
     for_each_nbr_bin(t.nb, tz, ty, tx, [&](int bin) { total += bin_start[bin + 1] - bin_start[bin]; });
-    if (total <= maxp) return;
-    const int64_t nsub = (total + maxp - 1) / maxp;
-    const int k = nsub <= 2 ? 0 : (nsub <= 4 ? 1 : 2);
-    const int pos = atomicAdd(&cnt[k], 1);
-    lists[(int64_t)k * ntiles + pos] = (int)tile;
+    cnt[tile] = total > maxp ? (int)((total + maxp - 1) / maxp) : 0;
+}
+
+__global__ void k_tile_parts_fill(const int* cnt, const int* off, int64_t ntiles, int4* parts) {
+    const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= ntiles) return;
+    const int n = cnt[tile], o = off[tile];
+    for (int q = 0; q < n; ++q) parts[o + q] = make_int4((int)tile, q, n, o);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1268,26 +1272,37 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             if (!ca[ax] && p->su[ax] && M > 0) cudaMemsetAsync(p->su[ax], 0, sizeof(float) * M, s);
         if (p->type == 1 && p->lc) {
             if (p->maxp_auto) p->maxp = auto_subproblem(M, g);
-            if (p->dense_list == nullptr) {
-                if ((st = dev_alloc(p, (void**)&p->dense_list, sizeof(int) * 3 * std::max<int64_t>(p->nbins, 1),
-                                    "dense tile lists")) != HB_OK)
-                    break;
-                if ((st = dev_alloc(p, (void**)&p->d_dense_cnt, sizeof(int) * 4, "dense tile counts")) != HB_OK) break;
-            }
             TileNbr tn;
             for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
-            if ((e = cudaMemsetAsync(p->d_dense_cnt, 0, sizeof(int) * 4, s)) != cudaSuccess) {
-                set_error(std::string("setpts memset: ") + cudaGetErrorString(e));
+            k_tile_parts_count<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins, p->maxp, ecnt);
+            if ((st = check_launch("k_tile_parts_count")) != HB_OK) break;
+            if ((st = exclusive_scan_int(ecnt, eoff, p->nbins, s, p->tmp_sums)) != HB_OK) break;
+            int n_parts = 0;
+            if ((e = cudaMemcpyAsync(&n_parts, eoff + p->nbins, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+                set_error(std::string("setpts sync: ") + cudaGetErrorString(e));
                 st = HB_ERR_CUDA;
                 break;
             }
-            k_tile_classify<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins, p->maxp,
-                                                                              p->d_dense_cnt, p->dense_list);
-            if ((st = check_launch("k_tile_classify")) != HB_OK) break;
-            if ((e = cudaMemcpyAsync(p->n_dense, p->d_dense_cnt, sizeof(int) * 3, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
-                set_error(std::string("setpts copy: ") + cudaGetErrorString(e));
-                st = HB_ERR_CUDA;
-                break;
+            if (n_parts > p->parts_cap) {
+                if (p->dense_parts) cudaFree(p->dense_parts);
+                p->dense_parts = nullptr;
+                p->parts_cap = 0;
+                if ((st = dev_alloc(p, (void**)&p->dense_parts, sizeof(int4) * n_parts, "dense tile parts")) != HB_OK) break;
+                p->parts_cap = n_parts;
+            }
+            const size_t need = sizeof(float2) * (size_t)n_parts * g.T[0] * g.T[1] * g.T[2] * g.C;
+            if (need > p->scratch_cap) {
+                if (p->dense_scratch) cudaFree(p->dense_scratch);
+                p->dense_scratch = nullptr;
+                p->scratch_cap = 0;
+                if ((st = dev_alloc(p, (void**)&p->dense_scratch, need, "dense tile partials")) != HB_OK) break;
+                p->scratch_cap = need;
+            }
+            p->n_parts = n_parts;
+            if (n_parts > 0) {
+                k_tile_parts_fill<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(ecnt, eoff, p->nbins, p->dense_parts);
+                if ((st = check_launch("k_tile_parts_fill")) != HB_OK) break;
             }
             p->n_extra = 0;
         } else if (p->type == 1) {
@@ -1622,8 +1637,13 @@ void plan_free(NufftPlan* p) {
         if (p->tmp_u[ax]) cudaFree(p->tmp_u[ax]);
         p->tmp_u[ax] = nullptr;
     }
-    for (int** q : {&p->tmp_binid, &p->tmp_rank, &p->tmp_count, &p->tmp_ecnt, &p->tmp_eoff, &p->tmp_sums,
-                    &p->dense_list, &p->d_dense_cnt}) {
+    if (p->dense_parts) cudaFree(p->dense_parts);
+    if (p->dense_scratch) cudaFree(p->dense_scratch);
+    p->dense_parts = nullptr;
+    p->dense_scratch = nullptr;
+    p->parts_cap = 0;
+    p->scratch_cap = 0;
+    for (int** q : {&p->tmp_binid, &p->tmp_rank, &p->tmp_count, &p->tmp_ecnt, &p->tmp_eoff, &p->tmp_sums}) {
         if (*q) cudaFree(*q);
         *q = nullptr;
     }

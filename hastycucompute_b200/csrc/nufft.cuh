@@ -70,14 +70,16 @@ struct NufftPlan {
     bool maxp_auto = true;
     int wb[3] = {2, 4, 4};
     // lanes-on-transforms spreading (k_spread_lc): usable for this plan's shape (lc_ok), chosen
-    // (lc), its transform chunk, and the dense tiles of the current points grouped by cluster
-    // size K = 2, 4, 8
+    // (lc), its transform chunk; the parts of the dense tiles of the current points ({tile, part,
+    // parts of the tile, first scratch slot of the tile}) and the scratch their partial tiles
+    // go to (one tile of all transforms per part)
     bool lc = false;
     bool lc_ok = false;
     int lc_cc = 0;
-    int* dense_list = nullptr;   // [3][nbins]
-    int* d_dense_cnt = nullptr;  // [4]
-    int n_dense[3] = {0, 0, 0};
+    int4* dense_parts = nullptr;
+    int64_t n_parts = 0, parts_cap = 0;
+    float2* dense_scratch = nullptr;
+    size_t scratch_cap = 0;  // bytes
     size_t device_bytes = 0;
 };
 

@@ -15,14 +15,13 @@
 // the same for the whole warp, so a switch over it selects code whose cell range and tap indices
 // are compile-time constants.
 //
-// Dense tiles (more candidates than a subproblem holds) run as a thread-block cluster of K = 2, 4
-// or 8 CTAs: each CTA spreads 1/K of the candidates into registers, the partial tiles meet in
-// shared memory, and each CTA sums one K-th of the cells over the cluster's CTAs through
-// distributed shared memory in rank order before storing. No global atomics anywhere; every cell
-// is written exactly once and the sum order is fixed.
+// Dense tiles (more candidates than a subproblem holds, maxp) are spread in ceil(total / maxp)
+// parts, one CTA each, however many that is, so the k-space centre of radial and spiral
+// trajectories spreads over the whole GPU; each part writes its partial tile (all transforms) to a
+// scratch slot held by the plan, and a second kernel sums a tile's partial tiles in part order and
+// stores the cells. No atomics anywhere; every cell is written exactly once, the sum order is
+// fixed, and no sequential FP32 sum runs over more than maxp candidates.
 #pragma once
-
-#include <cooperative_groups.h>
 
 #include <algorithm>
 
@@ -48,11 +47,7 @@ struct LcShape {
     // staging buffer: values float2[chunk][CC] | weights float[chunk][kLcRec] | packed first cells
     static constexpr int kValF = kLcChunk * CC * 2;
     static constexpr int kBufF = kValF + kLcChunk * kLcRec + kLcChunk;
-    static constexpr int kPartF = CELLS * CC * 2;  // one partial tile (cluster reduction)
-    static size_t smem_bytes(bool cluster) {
-        const int region = cluster ? (2 * kBufF > kPartF ? 2 * kBufF : kPartF) : 2 * kBufF;
-        return sizeof(float) * (size_t)(kCoefFloats + region);
-    }
+    static size_t smem_bytes() { return sizeof(float) * (size_t)(kCoefFloats + 2 * kBufF); }
 };
 static_assert(LcShape<32, true>::THREADS == 512 && LcShape<8, true>::THREADS == 128, "tile shape");
 static_assert(LcShape<32, false>::THREADS == 512 && LcShape<8, false>::THREADS == 128, "tile shape");
@@ -91,12 +86,12 @@ __device__ __forceinline__ void lc_dispatch(int k, float (&ar)[4][8], float (&ai
 }
 #undef HB_LC_CASE
 
-// tile_list == nullptr: one CTA per tile (blockIdx.x); tiles with more than maxp candidates are
-// left to the cluster launches. Otherwise CTA blockIdx.x spreads part blockIdx.x % K of tile
-// tile_list[blockIdx.x / K] inside a cluster of K CTAs.
+// parts == nullptr: one CTA per tile (blockIdx.x), storing the tile; tiles with more than maxp
+// candidates are left to the parts launch. Otherwise CTA blockIdx.x spreads part e.y of e.z of
+// tile e.x (e = parts[blockIdx.x]) into scratch slot e.w + e.y ([slot][cell][C]).
 template <int CC, int W, bool D3>
 __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
-    k_spread_lc(const GridArgs a, const int* __restrict__ tile_list, int K) {
+    k_spread_lc(const GridArgs a, const int4* __restrict__ parts, float2* __restrict__ scratch) {
     using S = LcShape<CC, D3>;
     extern __shared__ float4 sm_f4[];
     float* coef = reinterpret_cast<float*>(sm_f4);
@@ -106,8 +101,8 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int grp = lane / CC, coil = lane % CC;
 
-    const int tile = tile_list ? tile_list[blockIdx.x / K] : (int)blockIdx.x;
-    const int part = tile_list ? (int)(blockIdx.x % K) : 0;
+    const int4 job = parts ? parts[blockIdx.x] : make_int4((int)blockIdx.x, 0, 1, 0);
+    const int tile = job.x, part = job.y, K = job.z;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int org0 = tz * S::T0, org1 = ty * S::T1, org2 = tx * S::T2;
     const int nf1 = g.nf[1], nf2 = g.nf[2];
@@ -149,8 +144,8 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
     __syncthreads();
     const int nbin = s_nbin;
     const int total = s_pref[nbin];
-    if (!tile_list) {
-        if (total > a.maxp) return;  // a cluster launch spreads this tile
+    if (!parts) {
+        if (total > a.maxp) return;  // the parts launch spreads this tile
         if (total == 0) {
             // no point reaches the tile: 16-byte zero stores (a tile row of T2 cells x C values is
             // contiguous and 16-byte aligned: T2 and the tile origin are multiples of 8)
@@ -310,79 +305,68 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
             __syncthreads();
         }
         const bool coil_ok = cc0 + coil < g.C;
-        if (K == 1) {
+        float2* dst = parts ? scratch + (int64_t)(job.w + part) * S::CELLS * g.C : nullptr;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int z = z0 + (D3 ? (r >> 1) : 0), y = y0g + (D3 ? (r & 1) : r);
-                float2* row = a.grid + (((int64_t)(org0 + z) * nf1 + (org1 + y)) * nf2 + org2 + x0) * g.C + cc0 + coil;
-                if (coil_ok) {
+        for (int r = 0; r < 4; ++r) {
+            const int z = z0 + (D3 ? (r >> 1) : 0), y = y0g + (D3 ? (r & 1) : r);
+            float2* row = parts ? dst + ((int64_t)(z * S::T1 + y) * S::T2 + x0) * g.C + cc0 + coil
+                                : a.grid + (((int64_t)(org0 + z) * nf1 + (org1 + y)) * nf2 + org2 + x0) * g.C + cc0 + coil;
+            if (coil_ok) {
 #pragma unroll
-                    for (int x = 0; x < 8; ++x) row[(int64_t)x * g.C] = make_float2(ar[r][x], ai[r][x]);
-                }
+                for (int x = 0; x < 8; ++x) row[(int64_t)x * g.C] = make_float2(ar[r][x], ai[r][x]);
             }
-        } else {
-            // partial tiles meet in shared memory; CTA `part` sums cells [part, part+1) * CELLS / K
-            namespace cgx = cooperative_groups;
-            cgx::cluster_group cluster = cgx::this_cluster();
-            float2* ptile = reinterpret_cast<float2*>(region);
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const int z = z0 + (D3 ? (r >> 1) : 0), y = y0g + (D3 ? (r & 1) : r);
-#pragma unroll
-                for (int x = 0; x < 8; ++x)
-                    ptile[((z * S::T1 + y) * S::T2 + x0 + x) * CC + coil] = make_float2(ar[r][x], ai[r][x]);
-            }
-            cluster.sync();
-            const int per = S::CELLS * CC / K;
-            for (int i = part * per + tid; i < (part + 1) * per; i += S::THREADS) {
-                float2 sum = make_float2(0.f, 0.f);
-                for (int k2 = 0; k2 < K; ++k2) {
-                    const float2* rt = cluster.map_shared_rank(ptile, k2);
-                    const float2 v = rt[i];
-                    sum.x += v.x;
-                    sum.y += v.y;
-                }
-                const int c = i % CC, cell = i / CC;
-                if (cc0 + c < g.C) {
-                    const int x = cell % S::T2, y = (cell / S::T2) % S::T1, z = cell / (S::T2 * S::T1);
-                    a.grid[(((int64_t)(org0 + z) * nf1 + (org1 + y)) * nf2 + org2 + x) * g.C + cc0 + c] = sum;
-                }
-            }
-            cluster.sync();  // the partial tiles stay readable until every CTA has summed its share
         }
     }
 }
 
-// Host launch: one CTA per tile for the tiles within one subproblem, then one cluster launch per
-// cluster size for the dense tiles.
+// Sums the partial tiles of the dense tiles: CTA blockIdx.x takes entry e = parts[blockIdx.x] and
+// sums the e.z slots e.w .. e.w + e.z - 1 of tile e.x, in slot order, for its share (part e.y of
+// e.z) of the tile's cells x transforms, then stores them in the fine grid.
+template <bool D3>
+__global__ void __launch_bounds__(256) k_spread_lc_reduce(const GridArgs a, const int4* __restrict__ parts,
+                                                          const float2* __restrict__ scratch) {
+    using S = LcShape<32, D3>;
+    const GridGeom& g = a.g;
+    const int4 e = parts[blockIdx.x];
+    const int tile = e.x;
+    const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
+    const int org0 = tz * S::T0, org1 = ty * S::T1, org2 = tx * S::T2;
+    const int64_t E = (int64_t)S::CELLS * g.C;
+    const int64_t i0 = e.y * E / e.z, i1 = (e.y + 1) * E / e.z;
+    const float2* src = scratch + (int64_t)e.w * E;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        float2 sum = src[i];
+        for (int q = 1; q < e.z; ++q) {
+            const float2 v = src[(int64_t)q * E + i];
+            sum.x += v.x;
+            sum.y += v.y;
+        }
+        const int64_t cell = i / g.C;
+        const int c = (int)(i - cell * g.C);
+        const int x = (int)(cell % S::T2), y = (int)((cell / S::T2) % S::T1), z = (int)(cell / (S::T2 * S::T1));
+        a.grid[(((int64_t)(org0 + z) * g.nf[1] + (org1 + y)) * g.nf[2] + org2 + x) * g.C + c] = sum;
+    }
+}
+
+// Host launch: one CTA per tile for the tiles within one subproblem, then (dense tiles) one CTA per
+// part into scratch and the reduction of the parts.
 template <int CC, int W, bool D3>
 inline int launch_spread_lc(const NufftPlan* p, const GridArgs& a, cudaStream_t s) {
     using S = LcShape<CC, D3>;
     auto kern = k_spread_lc<CC, W, D3>;
-    const size_t sm_plain = S::smem_bytes(false), sm_cluster = S::smem_bytes(true);
-    HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max(sm_plain, sm_cluster)));
+    const size_t smem = S::smem_bytes();
+    HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     {
         TimedSection ts("spread", s);
-        kern<<<(unsigned)p->nbins, S::THREADS, sm_plain, s>>>(a, nullptr, 1);
+        kern<<<(unsigned)p->nbins, S::THREADS, smem, s>>>(a, nullptr, nullptr);
         HB_TRY(check_launch("k_spread_lc"));
     }
-    for (int k = 0; k < 3; ++k) {
-        if (p->n_dense[k] == 0) continue;
-        const int K = 2 << k;
+    if (p->n_parts > 0) {
         TimedSection ts("spread_dense", s);
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(K * p->n_dense[k]), 1, 1);
-        cfg.blockDim = dim3(S::THREADS, 1, 1);
-        cfg.dynamicSmemBytes = sm_cluster;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = (unsigned)K;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        HB_CUDA(cudaLaunchKernelEx(&cfg, kern, a, (const int*)(p->dense_list + (int64_t)k * p->nbins), K));
+        kern<<<(unsigned)p->n_parts, S::THREADS, smem, s>>>(a, p->dense_parts, p->dense_scratch);
+        HB_TRY(check_launch("k_spread_lc(parts)"));
+        k_spread_lc_reduce<D3><<<(unsigned)p->n_parts, 256, 0, s>>>(a, p->dense_parts, p->dense_scratch);
+        HB_TRY(check_launch("k_spread_lc_reduce"));
     }
     return HB_OK;
 }

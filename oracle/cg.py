@@ -19,6 +19,23 @@ def _rdot(a, b) -> float:
     return float(np.sum(a.real.astype(np.float64) * b.real + a.imag.astype(np.float64) * b.imag))
 
 
+def cg_iteration(A, x, r, p, rzold=None):
+    """One iteration of the recurrence above (cpp/corelib/lib/op/cg.cppm:139-150) from the state
+    (x, r, p) in FP64: returns (x', r', p', rznew)."""
+    x = np.asarray(x, dtype=np.complex128)
+    r = np.asarray(r, dtype=np.complex128)
+    p = np.asarray(p, dtype=np.complex128)
+    if rzold is None:
+        rzold = _rdot(r, r)
+    Ap = np.asarray(A(p), dtype=np.complex128)
+    alpha = rzold / _rdot(p, Ap)
+    x = x + alpha * p
+    r = r - alpha * Ap
+    rznew = _rdot(r, r)
+    p = r + (rznew / rzold) * p
+    return x, r, p, rznew
+
+
 def conjugate_gradient(A, b, x0, max_iter: int, tol: float = 1e-6, dtype=np.complex128):
     x = np.array(x0, dtype=dtype)
     b = np.asarray(b, dtype=dtype)

@@ -1,8 +1,8 @@
 """Type-1 spreading with the transforms on the lanes (3-D 8^3 and 2-D 16x32 tiles, widths 4..8,
 five or more transforms): parity with the FP64 gridding oracle (relative L2 <= 1e-5) for every
 transform chunk (8, 16, 32 lanes and more than 32 transforms), every width, both dimensions,
-periodic wrap at the grid edge, dense tiles spread by thread-block clusters of 2, 4 and 8 CTAs,
-and bit-identical repeats (the cluster sums run in a fixed order)."""
+periodic wrap at the grid edge, dense tiles spread in parts whose partial tiles a second kernel
+sums, and bit-identical repeats (the part sums run in a fixed order)."""
 import numpy as np
 import pytest
 
@@ -79,9 +79,10 @@ def test_lanes_on_transforms_periodic_edges(cuda, dim):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("dim,T,maxp", [(3, 32, None), (3, 32, 64), (3, 12, 32), (2, 12, 64), (3, 8, 128)])
-def test_lanes_on_transforms_dense_tiles_by_clusters(cuda, dim, T, maxp):
-    """Most points in a small ball around k = 0: the centre tiles hold several subproblems and
-    are spread by clusters of 2, 4 and 8 CTAs whose partial tiles are summed in shared memory."""
+def test_lanes_on_transforms_dense_tiles_in_parts(cuda, dim, T, maxp):
+    """Most points in a small ball around k = 0: the centre tiles hold many subproblems, each
+    spread by its own CTA into a scratch slot; the partial tiles are summed in part order. The
+    cells-on-lanes kernel gives the same transform."""
     import hastycucompute_b200 as hb
     rng = np.random.default_rng(31 + T + dim)
     nmodes = (32, 32, 32)[-dim:]
