@@ -126,13 +126,13 @@ int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block
     })
 }
 
-int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind) {
+int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind, int transforms_per_cta) {
     HB_GUARD({
         if (!plan) {
             hb::set_error("plan is null");
             return HB_ERR_INVALID_ARG;
         }
-        return hb::plan_set_spread_kernel(&plan->p, kind);
+        return hb::plan_set_spread_kernel(&plan->p, kind, transforms_per_cta);
     })
 }
 

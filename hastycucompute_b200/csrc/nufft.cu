@@ -1587,14 +1587,18 @@ int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx) {
     return HB_OK;
 }
 
-int plan_set_spread_kernel(NufftPlan* p, int kind) {
+int plan_set_spread_kernel(NufftPlan* p, int kind, int transforms_per_cta) {
     HB_REQUIRE(!p->pts_set, HB_ERR_STATE, "set the spreading kernel before setpts");
-    HB_REQUIRE(kind == HB_SPREAD_AUTO || kind == HB_SPREAD_CELLS || kind == HB_SPREAD_TRANSFORMS, HB_ERR_INVALID_ARG,
+    const int base = kind;
+    HB_REQUIRE(base == HB_SPREAD_AUTO || base == HB_SPREAD_CELLS || base == HB_SPREAD_TRANSFORMS, HB_ERR_INVALID_ARG,
                "spreading kernel must be HB_SPREAD_AUTO, HB_SPREAD_CELLS or HB_SPREAD_TRANSFORMS");
-    HB_REQUIRE(kind != HB_SPREAD_TRANSFORMS || p->lc_ok, HB_ERR_INVALID_ARG,
+    HB_REQUIRE(base != HB_SPREAD_TRANSFORMS || p->lc_ok, HB_ERR_INVALID_ARG,
                "this plan cannot spread with the transforms on the lanes (needs 8^3 / 16x32 tiles, width 4..8, "
                ">= 5 transforms, >= 2 tiles per axis)");
-    p->lc = kind == HB_SPREAD_CELLS ? false : p->lc_ok;
+    HB_REQUIRE(transforms_per_cta == 0 || transforms_per_cta == 8 || transforms_per_cta == 16 || transforms_per_cta == 32,
+               HB_ERR_INVALID_ARG, "transforms per CTA must be 0 (automatic), 8, 16 or 32");
+    p->lc = base == HB_SPREAD_CELLS ? false : p->lc_ok;
+    if (transforms_per_cta) p->lc_cc = transforms_per_cta;
     return HB_OK;
 }
 

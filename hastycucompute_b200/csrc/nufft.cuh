@@ -112,7 +112,7 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
 int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s);
 int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s);
 int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx);
-int plan_set_spread_kernel(NufftPlan* p, int kind);
+int plan_set_spread_kernel(NufftPlan* p, int kind, int transforms_per_cta);
 void plan_free(NufftPlan* p);
 
 // Pieces reused by the Toeplitz kernel builder.

@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
     if (!parts) {
         if (total > a.maxp) return;  // the parts launch spreads this tile
         if (total == 0) {
+            if (blockIdx.y != 0) return;
             // no point reaches the tile: 16-byte zero stores (a tile row of T2 cells x C values is
             // contiguous and 16-byte aligned: T2 and the tile origin are multiples of 8)
             const int rowf4 = (S::T2 * g.C) >> 1;
@@ -177,66 +178,85 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
         return s_start[b] + (k - s_pref[b]);
     };
 
+    // Stages candidates base .. base+n-1: thread (q, axis) finds candidate q's sorted index once,
+    // folds all three coordinates to tile-relative first cells, and -- only when the footprint
+    // reaches the tile along every axis (about half of the lower neighbours' points do not) --
+    // writes its axis's weights and a third of the point's CC values (cp.async). A point that
+    // misses the tile is marked so no warp visits it.
     auto stage = [&](int base, int cc0, float* buf) {
         const int n = min(kLcChunk, k_end - base);
         float2* bval = reinterpret_cast<float2*>(buf);
         float* bwt = buf + S::kValF;
         unsigned char* brel = reinterpret_cast<unsigned char*>(bwt + kLcChunk * kLcRec);
-        constexpr int CP = CC / 2;
-        for (int i = tid; i < n * CP; i += S::THREADS) {
-            const int q = i / CP, c = 2 * (i % CP);
-            float2* dst = bval + q * CC + c;
-            const int cg = cc0 + c;
-            const float2* src = a.inT + (int64_t)a.perm[sorted_index(base + q)] * g.C + cg;
-            if (vec && cg < g.C) {
-                cp_async16(dst, src);
-            } else {
-                if (cg < g.C) cp_async8(dst, src); else dst[0] = make_float2(0.f, 0.f);
-                if (cg + 1 < g.C) cp_async8(dst + 1, src + 1); else dst[1] = make_float2(0.f, 0.f);
-            }
-        }
+        constexpr int CP = CC / 2;               // 16-byte pieces of a point's values
+        constexpr int PPA = (CP + 2) / 3;        // pieces per axis thread
         for (int i = tid; i < 3 * n; i += S::THREADS) {
             const int q = i / 3, ax = i - 3 * q;
-            float* rec = bwt + q * kLcRec;
-            int rel = 0;
-            if (ax == 0 && !D3) {
-                rec[0] = 1.f;
+            const int sidx = sorted_index(base + q);
+            int rel[3];
+            bool reach = true;
 #pragma unroll
-                for (int d = 1; d < 8; ++d) rec[d] = 0.f;
-            } else {
-                const float u = a.su[ax][sorted_index(base + q)];
-                const float v = __fsub_rn(u, hw);
-                const int ic = (int)ceilf(v);
-                const float sarg = fmaf(2.f, __fsub_rn((float)ic, v), -1.f);
-                const int nf = g.nf[ax];
-                const int T = ax == 0 ? S::T0 : (ax == 1 ? S::T1 : S::T2);
-                int iw = ic;
+            for (int a3 = 0; a3 < 3; ++a3) {
+                rel[a3] = 0;
+                if (a3 == 0 && !D3) continue;
+                const int T = a3 == 0 ? S::T0 : (a3 == 1 ? S::T1 : S::T2);
+                const int nf = g.nf[a3];
+                int iw = (int)ceilf(__fsub_rn(a.su[a3][sidx], hw));
                 if (iw < 0) iw += nf;
                 if (iw >= nf) iw -= nf;
-                rel = iw - (ax == 0 ? org0 : (ax == 1 ? org1 : org2));
-                if (rel < 0) rel += nf;
-                if (rel >= T) rel -= nf;  // a footprint reaching the tile from below starts at -(W-1) .. -1
+                int r = iw - (a3 == 0 ? org0 : (a3 == 1 ? org1 : org2));
+                if (r < 0) r += nf;
+                if (r >= T) r -= nf;  // a footprint reaching the tile from below starts at -(W-1) .. -1
+                rel[a3] = r;
+                reach = reach && r >= -(W - 1);
+            }
+            if (ax == 0)
+                *reinterpret_cast<int*>(brel + q * 4) =
+                    reach ? (rel[0] + 16) | ((rel[1] + 16) << 8) | ((rel[2] + 16) << 16) : 0;
+            if (!reach) continue;
+            float* rec = bwt + q * kLcRec;
+            if (ax == 0 && !D3) {
+                reinterpret_cast<float4*>(rec)[0] = make_float4(1.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<float4*>(rec)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                const float v = __fsub_rn(a.su[ax][sidx], hw);
+                const float sarg = fmaf(2.f, __fsub_rn(ceilf(v), v), -1.f);
                 float t[W];
 #pragma unroll
                 for (int d = 0; d < W; ++d) t[d] = kb_tap(coef, a.kb.deg, d, sarg);
                 if (ax == 2) {
-#pragma unroll
-                    for (int d = 0; d < 8; ++d) rec[24 + d] = d < W ? t[d] : 0.f;
+                    reinterpret_cast<float4*>(rec + 24)[0] = make_float4(t[0], t[1], t[2], t[3]);
+                    reinterpret_cast<float4*>(rec + 24)[1] =
+                        make_float4(W > 4 ? t[4 % W] : 0.f, W > 5 ? t[5 % W] : 0.f, W > 6 ? t[6 % W] : 0.f,
+                                    W > 7 ? t[7 % W] : 0.f);
                 } else {
+                    const int T = ax == 0 ? S::T0 : S::T1;
                     float* wt = rec + (ax == 0 ? 0 : 8);
-                    for (int c = 0; c < T; ++c) wt[c] = 0.f;
+                    const int r = rel[ax];
+                    for (int c = 0; c < T; c += 4) *reinterpret_cast<float4*>(wt + c) = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                     for (int d = 0; d < W; ++d) {
-                        const int c = rel + d;
+                        const int c = r + d;
                         if (c >= 0 && c < T) wt[c] = t[d];
                     }
                 }
             }
-            brel[q * 4 + ax] = (unsigned char)max(min(rel + 16, 255), 0);
+            const float2* src = a.inT + (int64_t)a.perm[sidx] * g.C;
+            for (int pc = ax * PPA; pc < min(CP, (ax + 1) * PPA); ++pc) {
+                const int c = 2 * pc, cg = cc0 + c;
+                float2* dst = bval + q * CC + c;
+                if (vec && cg < g.C) {
+                    cp_async16(dst, src + cg);
+                } else {
+                    if (cg < g.C) cp_async8(dst, src + cg); else dst[0] = make_float2(0.f, 0.f);
+                    if (cg + 1 < g.C) cp_async8(dst + 1, src + cg + 1); else dst[1] = make_float2(0.f, 0.f);
+                }
+            }
         }
     };
 
-    for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
+    {
+        const int cc0 = (int)blockIdx.y * CC;  // this CTA's transform chunk
         float ar[4][8], ai[4][8];
 #pragma unroll
         for (int r = 0; r < 4; ++r)
@@ -294,10 +314,12 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
                             ur[r] = rw[r] * v.x;
                             ui[r] = rw[r] * v.y;
                         }
-                        const float4 xa = *reinterpret_cast<const float4*>(rec + 24);
-                        const float4 xb = *reinterpret_cast<const float4*>(rec + 28);
-                        const float wx[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-                        lc_dispatch<W>(k, ar, ai, wx, ur, ui);
+                        {
+                            const float4 xa = *reinterpret_cast<const float4*>(rec + 24);
+                            const float4 xb = *reinterpret_cast<const float4*>(rec + 28);
+                            const float wx[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+                            lc_dispatch<W>(k, ar, ai, wx, ur, ui);
+                        }
                     }
                 }
             }
@@ -358,12 +380,13 @@ inline int launch_spread_lc(const NufftPlan* p, const GridArgs& a, cudaStream_t 
     HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     {
         TimedSection ts("spread", s);
-        kern<<<(unsigned)p->nbins, S::THREADS, smem, s>>>(a, nullptr, nullptr);
+        kern<<<dim3((unsigned)p->nbins, (unsigned)ceil_div(a.g.C, CC)), S::THREADS, smem, s>>>(a, nullptr, nullptr);
         HB_TRY(check_launch("k_spread_lc"));
     }
     if (p->n_parts > 0) {
         TimedSection ts("spread_dense", s);
-        kern<<<(unsigned)p->n_parts, S::THREADS, smem, s>>>(a, p->dense_parts, p->dense_scratch);
+        kern<<<dim3((unsigned)p->n_parts, (unsigned)ceil_div(a.g.C, CC)), S::THREADS, smem, s>>>(
+            a, p->dense_parts, p->dense_scratch);
         HB_TRY(check_launch("k_spread_lc(parts)"));
         k_spread_lc_reduce<D3><<<(unsigned)p->n_parts, 256, 0, s>>>(a, p->dense_parts, p->dense_scratch);
         HB_TRY(check_launch("k_spread_lc_reduce"));

@@ -162,13 +162,14 @@ class NufftPlan:
             b = (1,) + b
         _lib.call("hb_nufft_set_spread_tuning", self._h, int(max_candidates), *b)
 
-    def set_spread_kernel(self, kind: str = "auto") -> None:
+    def set_spread_kernel(self, kind: str = "auto", transforms_per_cta: int = 0) -> None:
         """Spreading kernel (before setpts): "auto", "cells" (one cell per lane) or "transforms"
-        (transforms on the lanes). All compute the same sums."""
+        (transforms on the lanes), and for the latter the transforms one CTA spreads (8, 16, 32;
+        0 = automatic). All compute the same sums."""
         if self.M is not None:
             raise RuntimeError("set the spreading kernel before setpts")
         code = {"auto": 0, "cells": 1, "transforms": 2}[kind]
-        _lib.call("hb_nufft_set_spread_kernel", self._h, code)
+        _lib.call("hb_nufft_set_spread_kernel", self._h, code, int(transforms_per_cta))
 
     def info(self) -> PlanInfo:
         fine = (C.c_int64 * 3)()

@@ -109,11 +109,13 @@ int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block
  * HB_SPREAD_AUTO (transforms on the lanes when the plan allows it: 8^3 or 16x32 tiles, widths
  * 4..8, 5 or more transforms, two or more tiles per axis), HB_SPREAD_CELLS (one cell per lane,
  * any plan), HB_SPREAD_TRANSFORMS (transforms on the lanes; HB_ERR_INVALID_ARG where the plan
- * does not allow it). Every choice computes the same sums. */
+ * does not allow it). transforms_per_cta (8, 16 or 32; 0 = automatic) sets how many transforms
+ * one CTA of the transforms kernel spreads; larger transform counts run as several CTAs per tile.
+ * Every choice computes the same sums. */
 #define HB_SPREAD_AUTO       0
 #define HB_SPREAD_CELLS      1
 #define HB_SPREAD_TRANSFORMS 2
-int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind);
+int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind, int transforms_per_cta);
 
 /* Coordinate gradient (no counterpart in the reference, which has no derivatives): with a
  * type-2 plan (sign s) whose points are set, writes to grad ([dim][M] float, image order)
