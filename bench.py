@@ -755,7 +755,7 @@ def bench_configs(args, hb, dev, stream):
                       "peak_hbm_gb": round(peak / 1e9, 2), "resident_before_gb": round(base / 1e9, 2),
                       "aha_rel_err_vs_fp64_oracle": acc4,
                       "scalar_gradient_check": "tests/test_configs_gpu.py: the 20 learnable scalars at this size "
-                                               "vs central differences (h = 1e-2), <= 1e-3"}
+                                               "vs central differences with two Richardson steps, <= 1e-3"}
     del net, op4, Ks, S
     torch.cuda.empty_cache()
     return res
