@@ -31,7 +31,6 @@
 
 namespace hb {
 
-constexpr int kLcChunk = 128;  // candidates staged per chunk
 constexpr int kLcRec = 32;     // weight floats per staged point: wz_t[8] | wy_t[16] | wx[8]
 
 template <int CC, bool D3>
@@ -44,6 +43,9 @@ struct LcShape {
     static constexpr int WARPS = NZB * NYB * NXS;
     static constexpr int THREADS = WARPS * 32;
     static constexpr int CELLS = T0 * T1 * T2;
+    // candidates staged per chunk: the 32-transform CTA is alone on its SM (registers), so it
+    // takes long chunks (fewer barriers, even warp loads); smaller CTAs keep several per SM
+    static constexpr int kLcChunk = CC == 32 ? 256 : 128;
     // staging buffer: values float2[chunk][CC] | weights float[chunk][kLcRec] | packed first cells
     static constexpr int kValF = kLcChunk * CC * 2;
     static constexpr int kBufF = kValF + kLcChunk * kLcRec + kLcChunk;
@@ -184,10 +186,10 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
     // writes its axis's weights and a third of the point's CC values (cp.async). A point that
     // misses the tile is marked so no warp visits it.
     auto stage = [&](int base, int cc0, float* buf) {
-        const int n = min(kLcChunk, k_end - base);
+        const int n = min(S::kLcChunk, k_end - base);
         float2* bval = reinterpret_cast<float2*>(buf);
         float* bwt = buf + S::kValF;
-        unsigned char* brel = reinterpret_cast<unsigned char*>(bwt + kLcChunk * kLcRec);
+        unsigned char* brel = reinterpret_cast<unsigned char*>(bwt + S::kLcChunk * kLcRec);
         constexpr int CP = CC / 2;               // 16-byte pieces of a point's values
         constexpr int PPA = (CP + 2) / 3;        // pieces per axis thread
         for (int i = tid; i < 3 * n; i += S::THREADS) {
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
                 } else {
                     const int T = ax == 0 ? S::T0 : S::T1;
                     float* wt = rec + (ax == 0 ? 0 : 8);
-                    const int r = rel[ax];
+                    const int r = ax == 0 ? rel[0] : rel[1];
                     for (int c = 0; c < T; c += 4) *reinterpret_cast<float4*>(wt + c) = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                     for (int d = 0; d < W; ++d) {
@@ -262,21 +264,21 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
         for (int r = 0; r < 4; ++r)
 #pragma unroll
             for (int x = 0; x < 8; ++x) ar[r][x] = ai[r][x] = 0.f;
-        const int nch = (k_end - k_begin + kLcChunk - 1) / kLcChunk;
+        const int nch = (k_end - k_begin + S::kLcChunk - 1) / S::kLcChunk;
         if (nch > 0) stage(k_begin, cc0, region);
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
         for (int it = 0; it < nch; ++it) {
-            const int base = k_begin + it * kLcChunk;
-            if (it + 1 < nch) stage(base + kLcChunk, cc0, region + ((it + 1) & 1) * S::kBufF);
+            const int base = k_begin + it * S::kLcChunk;
+            if (it + 1 < nch) stage(base + S::kLcChunk, cc0, region + ((it + 1) & 1) * S::kBufF);
             cp_async_commit();
             {
-                const int n = min(kLcChunk, k_end - base);
+                const int n = min(S::kLcChunk, k_end - base);
                 const float* buf = region + (it & 1) * S::kBufF;
                 const float2* bval = reinterpret_cast<const float2*>(buf);
                 const float* bwt = buf + S::kValF;
-                const int* brel = reinterpret_cast<const int*>(bwt + kLcChunk * kLcRec);
+                const int* brel = reinterpret_cast<const int*>(bwt + S::kLcChunk * kLcRec);
                 for (int q0 = 0; q0 < n; q0 += 32) {
                     const int qq = q0 + lane;
                     bool hit = false;
