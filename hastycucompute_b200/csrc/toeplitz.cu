@@ -432,7 +432,18 @@ static int toep_run(const ToepGeom& t, const ToepArgs& a, float2* ws, cudaStream
     }
     // P5: axis 2 inverse, crop, output ops
     {
-        if (a.sense) {
+        if (a.sense && a.frames > 1) {
+            // frames: one launch per frame over that frame's coil columns, so a CTA sums one frame's
+            // coils of a row (one running sum in shared memory) instead of walking every frame's
+            // columns with a running sum per frame (measured at 24 frames x 16 coils x 128^3:
+            // 7.4 ms against 10.3 ms per apply)
+            for (int64_t f = 0; f < a.frames; ++f) {
+                OpToepOutSense op{W1 + f * cpf, (int64_t)L2 * B, B, a.smaps_out ? a.smaps_out : a.in, a.out + f * t.n,
+                                  N2, t.n, cpf, 1, a.odiag, a.accumulate};
+                HB_TRY(launch_fft_pass(op, f2, N0 * N1, cpf, L2, 0, (int)N2, 0, 1, sizeof(float2) * (size_t)N2, s,
+                                       "toeplitz P5 sense"));
+            }
+        } else if (a.sense) {
             OpToepOutSense op{W1,   (int64_t)L2 * B,   B,       a.smaps_out ? a.smaps_out : a.in, a.out, N2, t.n, cpf,
                               (int)a.frames, a.odiag, a.accumulate};
             HB_TRY(launch_fft_pass(op, f2, N0 * N1, B, L2, 0, (int)N2, 0, 1,
