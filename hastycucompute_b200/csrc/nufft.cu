@@ -769,7 +769,8 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
             // Common case: the footprint wraps neither along axis 2 nor axis 1 and the lanes hold
             // all C transforms, so a tap's column stride is the compile-time CC: one row pointer,
             // W loads at constant offsets.
-            const bool slab_fast = (W <= 6) && g.C == CC && wy == W && i0[2] + W <= nf2 && i0[1] + W <= nf1;
+            const bool slab_fast = (W <= 6) && g.C % CC == 0 && wy == W && i0[2] + W <= nf2 && i0[1] + W <= nf1;
+            const unsigned cs = (unsigned)g.C;  // column stride of a tap along axis 2
             for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
                 if (cc0 + coil >= g.C) break;
                 const float2* gridc = a.grid + cc0 + coil;
@@ -781,13 +782,13 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
                     if constexpr (W <= 6) {
                         if (slab_fast) {
                             const float2* p0 =
-                                gridc + (((unsigned)gz * (unsigned)nf1 + (unsigned)i0[1]) * (unsigned)nf2 + (unsigned)i0[2]) * (unsigned)CC;
+                                gridc + (((unsigned)gz * (unsigned)nf1 + (unsigned)i0[1]) * (unsigned)nf2 + (unsigned)i0[2]) * cs;
                             float2 v[W * W];
 #pragma unroll
                             for (int dy = 0; dy < W; ++dy) {
                                 const float2* pr = p0 + (size_t)dy * rowstride;
 #pragma unroll
-                                for (int dx = 0; dx < W; ++dx) v[dy * W + dx] = pr[dx * CC];
+                                for (int dx = 0; dx < W; ++dx) v[dy * W + dx] = pr[dx * (g.C == CC ? CC : cs)];
                             }
 #pragma unroll
                             for (int dy = 0; dy < W; ++dy) {
@@ -1540,7 +1541,7 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
         GridArgs a = grid_args(p);
         a.grid = G;
         a.out = out;
-        HB_TRY(dispatch_cc(spread_cc(g), p, a, s, false));
+        HB_TRY(dispatch_cc(p->interp_cc ? p->interp_cc : spread_cc(g), p, a, s, false));
     }
     return HB_OK;
 }
@@ -1599,6 +1600,15 @@ int plan_set_spread_kernel(NufftPlan* p, int kind, int transforms_per_cta) {
                HB_ERR_INVALID_ARG, "transforms per CTA must be 0 (automatic), 8, 16 or 32");
     p->lc = base == HB_SPREAD_CELLS ? false : p->lc_ok;
     if (transforms_per_cta) p->lc_cc = transforms_per_cta;
+    return HB_OK;
+}
+
+int plan_set_interp_tuning(NufftPlan* p, int transforms_per_group) {
+    HB_REQUIRE(transforms_per_group == 0 || transforms_per_group == 1 || transforms_per_group == 2 ||
+                   transforms_per_group == 4 || transforms_per_group == 8 || transforms_per_group == 16 ||
+                   transforms_per_group == 32,
+               HB_ERR_INVALID_ARG, "transforms per lane group must be 0 (automatic) or a power of two up to 32");
+    p->interp_cc = transforms_per_group;
     return HB_OK;
 }
 

@@ -76,6 +76,7 @@ struct NufftPlan {
     bool lc = false;
     bool lc_ok = false;
     int lc_cc = 0;
+    int interp_cc = 0;  // interpolation: transforms per lane group (0 = the spreading rule)
     int4* dense_parts = nullptr;
     int64_t n_parts = 0, parts_cap = 0;
     float2* dense_scratch = nullptr;
@@ -113,6 +114,7 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s);
 int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s);
 int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx);
 int plan_set_spread_kernel(NufftPlan* p, int kind, int transforms_per_cta);
+int plan_set_interp_tuning(NufftPlan* p, int transforms_per_group);
 void plan_free(NufftPlan* p);
 
 // Pieces reused by the Toeplitz kernel builder.

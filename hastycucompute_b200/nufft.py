@@ -171,6 +171,11 @@ class NufftPlan:
         code = {"auto": 0, "cells": 1, "transforms": 2}[kind]
         _lib.call("hb_nufft_set_spread_kernel", self._h, code, int(transforms_per_cta))
 
+    def set_interp_tuning(self, transforms_per_group: int = 0) -> None:
+        """Interpolation (type 2): transforms per lane group (points per warp = 32 / that; 0 =
+        automatic). All choices compute the same sums."""
+        _lib.call("hb_nufft_set_interp_tuning", self._h, int(transforms_per_group))
+
     def info(self) -> PlanInfo:
         fine = (C.c_int64 * 3)()
         w = C.c_int()

@@ -117,6 +117,11 @@ int hb_nufft_set_spread_tuning(hb_nufft_plan plan, int max_candidates, int block
 #define HB_SPREAD_TRANSFORMS 2
 int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind, int transforms_per_cta);
 
+/* Interpolation of a type-2 plan (no counterpart in the reference): the transforms one group of
+ * lanes gathers per point (1, 2, 4, 8, 16 or 32; 0 = automatic), i.e. 32 / that many points per
+ * warp in flight at once. Every choice computes the same sums. */
+int hb_nufft_set_interp_tuning(hb_nufft_plan plan, int transforms_per_group);
+
 /* Coordinate gradient (no counterpart in the reference, which has no derivatives): with a
  * type-2 plan (sign s) whose points are set, writes to grad ([dim][M] float, image order)
  *   grad[i][j] = -(nf_i / 2 pi) Re( sum_c h[c][j] sum_l G_c[l] dPhi_i(l - u_j) )

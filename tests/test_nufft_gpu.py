@@ -268,3 +268,19 @@ def test_upsampfac_1_25(cuda, dim, nmodes, M, T, w):
     p2 = hb.NufftPlan(hb.NufftType.TYPE_2, opts)
     p2.setpts([to_dev(x, cuda) for x in coords])
     assert relerr(to_np(p2(to_dev(f, cuda))), gridding.nufft2(coords, f, w=w, sigma=1.25)) <= PARITY
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nmodes,T,w", [((20, 24, 16), 32, 6), ((24, 20, 16), 16, 4), ((40, 36), 12, 4)])
+@pytest.mark.parametrize("per_group", [0, 32, 16, 8, 4])
+def test_interp_lane_groups_agree(cuda, nmodes, T, w, per_group):
+    """hb_nufft_set_interp_tuning: every lane-group size gathers the same sums (vs the oracle)."""
+    import hastycucompute_b200 as hb
+    rng = np.random.default_rng(T + w + per_group)
+    M = 5000
+    coords = rand_coords(rng, len(nmodes), M)
+    f = crand(rng, T, *nmodes)
+    p = hb.NufftPlan(hb.NufftType.TYPE_2, hb.NufftOpts(nmodes=nmodes, ntransf=T, kernel_width=w))
+    p.set_interp_tuning(per_group)
+    p.setpts([to_dev(x, cuda) for x in coords])
+    assert relerr(to_np(p(to_dev(f, cuda))), gridding.nufft2(coords, f, w=w)) <= PARITY
