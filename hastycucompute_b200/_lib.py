@@ -38,6 +38,7 @@ SIGNATURES = {
     "hb_nufft_set_spread_tuning": (_i, [_vp, _i, _i, _i, _i]),
     "hb_nufft_set_spread_kernel": (_i, [_vp, _i, _i]),
     "hb_nufft_set_interp_tuning": (_i, [_vp, _i]),
+    "hb_nufft_set_interp_kernel": (_i, [_vp, _i]),
     "hb_nufft_get_info": (_i, [_vp, _pi64, C.POINTER(_i), C.POINTER(_d), C.POINTER(_sz)]),
     "hb_toeplitz_kernel": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "hb_transform_toeplitz_kernel": (_i, [_i, _pi64, _vp, _vp, _vp]),

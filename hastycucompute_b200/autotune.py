@@ -1,13 +1,17 @@
-"""Spreading autotuner: picks the spreading kernel, its cell block and the points per spread
-subproblem for a given problem by timing type-1 plans on the device, and caches the choice as JSON.
+"""Gridding autotuner: picks the spreading kernel, its cell block and the points per spread
+subproblem for a given problem by timing type-1 plans on the device, and the interpolation lane
+groups by timing type-2 plans, and caches the choices as JSON.
 
-Search space (all exact, all give the same result up to float rounding):
+Spreading search space (all exact, all give the same result up to float rounding):
 - the kernel: transforms on the lanes (each thread owns 4 rows x 8 cells of one transform; dense
-  tiles go to thread-block clusters of 2/4/8 CTAs) or cells on the lanes (each thread owns one
-  cell; dense tiles as extra subproblems);
+  tiles are spread in parts whose partial tiles a second kernel sums) or cells on the lanes (each
+  thread owns one cell; dense tiles as extra subproblems);
 - for cells on the lanes, the 32-cell block each warp owns inside a spread tile: 3-D tiles are
   8x8x8, so any (bz, by, bx) with bz*by*bx = 32 and each edge dividing 8; 2-D tiles are 16x32;
 - points per subproblem (when a tile is dense enough to split): 256 .. 8192.
+
+Interpolation search space: the transforms a lane group gathers per point (32, 16, 8 or 4 lanes;
+all give bit-identical results).
 
 Cache key: dimensionality, modes, transforms, kernel width, number of points and a coarse
 density signature of the trajectory (quartiles of |k|), so the same trajectory family reuses the
@@ -109,7 +113,56 @@ def tune_spread(nmodes: Sequence[int], ntransf: int, coords: Sequence[torch.Tens
     return dict(best, cached=False)
 
 
+INTERP_GROUPS = [32, 16, 8, 4]
+
+
+def tune_interp(nmodes: Sequence[int], ntransf: int, coords: Sequence[torch.Tensor], kernel_width: int,
+                reps: int = 3, use_cache: bool = True) -> dict:
+    """Times type-2 executes over the interpolation lane-group sizes; returns {"interp_group",
+    "ms", "timings"} for the fastest and stores it in the cache."""
+    nmodes = tuple(int(n) for n in nmodes)
+    key = "interp|" + _key(nmodes, ntransf, kernel_width, coords)
+    cache = _load() if use_cache else {}
+    if key in cache:
+        return dict(cache[key], cached=True)
+    dev = coords[0].device
+    M = coords[0].shape[0]
+    img = torch.randn((ntransf, *nmodes), dtype=torch.complex64, device=dev)
+    out = torch.empty((ntransf, M), dtype=torch.complex64, device=dev)
+    timings = []
+    for grp in INTERP_GROUPS:
+        plan = NufftPlan(NufftType.TYPE_2, NufftOpts(nmodes=nmodes, ntransf=ntransf, kernel_width=kernel_width))
+        try:
+            plan.set_interp_tuning(grp)
+        except Exception:
+            plan.free()
+            continue
+        plan.setpts(list(coords))
+        plan.execute(img, out)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            plan.execute(img, out)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        timings.append((e0.elapsed_time(e1) / reps, grp))
+        plan.free()
+    timings.sort(key=lambda r: r[0])
+    best = {"interp_group": int(timings[0][1]), "ms": round(timings[0][0], 4),
+            "timings": [[round(t, 4), g] for t, g in timings]}
+    if use_cache:
+        cache = _load()
+        cache[key] = best
+        _store(cache)
+    return dict(best, cached=False)
+
+
 def apply(plan: NufftPlan, choice: dict) -> None:
-    """Applies a tuner choice to a plan (before its setpts)."""
-    plan.set_spread_kernel(choice.get("kernel", "auto"))
-    plan.set_spread_tuning(int(choice["max_candidates"]), tuple(choice["block"]))
+    """Applies a tuner choice (from tune_spread, tune_interp or both merged) to a plan, before its
+    setpts."""
+    if "max_candidates" in choice:
+        plan.set_spread_kernel(choice.get("kernel", "auto"))
+        plan.set_spread_tuning(int(choice["max_candidates"]), tuple(choice["block"]))
+    if "interp_group" in choice:
+        plan.set_interp_tuning(int(choice["interp_group"]))

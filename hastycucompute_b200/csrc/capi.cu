@@ -146,6 +146,16 @@ int hb_nufft_set_interp_tuning(hb_nufft_plan plan, int transforms_per_group) {
     })
 }
 
+int hb_nufft_set_interp_kernel(hb_nufft_plan plan, int kind) {
+    HB_GUARD({
+        if (!plan) {
+            hb::set_error("plan is null");
+            return HB_ERR_INVALID_ARG;
+        }
+        return hb::plan_set_interp_kernel(&plan->p, kind);
+    })
+}
+
 int hb_nufft_coord_grad(hb_nufft_plan plan, const void* modes, const void* h, float* grad, void* stream) {
     HB_GUARD({
         if (!plan) {

@@ -1133,6 +1133,8 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
         for (int ax = 3 - dim; ax < 3; ++ax) ok = ok && g.nb[ax] >= 2;
         p->lc = p->lc_ok = ok;
         p->lc_cc = ntransf >= 17 ? 32 : (ntransf >= 9 ? 16 : 8);
+        p->st_ok = type == 2 && dim == 3 && w >= 4 && w <= 7;
+        p->st = false;
     }
     p->beta = kb_beta(w, p->sigma);
     const double fit_err = kb_fit(&p->kb, w, p->beta);
@@ -1339,6 +1341,24 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
                 if ((st = check_launch("k_tile_extra_fill")) != HB_OK) break;
             }
         }
+        if (p->type == 2 && p->st_ok) {
+            int n_jobs = 0;
+            if ((st = interp_st_jobs(p->bin_start, p->nbins, g.wa[2], ecnt, eoff, p->tmp_sums, nullptr, &n_jobs, 0, s)) !=
+                HB_OK)
+                break;
+            if (n_jobs > p->st_cap) {
+                if (p->st_jobs) cudaFree(p->st_jobs);
+                p->st_jobs = nullptr;
+                p->st_cap = 0;
+                if ((st = dev_alloc(p, (void**)&p->st_jobs, sizeof(int4) * n_jobs, "staged interpolation jobs")) != HB_OK)
+                    break;
+                p->st_cap = n_jobs;
+            }
+            if ((st = interp_st_jobs(p->bin_start, p->nbins, g.wa[2], ecnt, eoff, p->tmp_sums, p->st_jobs, &n_jobs,
+                                     p->st_cap, s)) != HB_OK)
+                break;
+            p->n_st_jobs = n_jobs;
+        }
         {
             int err = 0;
             if ((e = cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
@@ -1541,7 +1561,10 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
         GridArgs a = grid_args(p);
         a.grid = G;
         a.out = out;
-        HB_TRY(dispatch_cc(p->interp_cc ? p->interp_cc : spread_cc(g), p, a, s, false));
+        if (p->st)
+            HB_TRY(interp_st_run(p, a, s));
+        else
+            HB_TRY(dispatch_cc(p->interp_cc ? p->interp_cc : spread_cc(g), p, a, s, false));
     }
     return HB_OK;
 }
@@ -1612,6 +1635,15 @@ int plan_set_interp_tuning(NufftPlan* p, int transforms_per_group) {
     return HB_OK;
 }
 
+int plan_set_interp_kernel(NufftPlan* p, int kind) {
+    HB_REQUIRE(kind == HB_INTERP_AUTO || kind == HB_INTERP_GATHER || kind == HB_INTERP_STAGED, HB_ERR_INVALID_ARG,
+               "interpolation kernel must be HB_INTERP_AUTO, HB_INTERP_GATHER or HB_INTERP_STAGED");
+    HB_REQUIRE(kind != HB_INTERP_STAGED || p->st_ok, HB_ERR_INVALID_ARG,
+               "staged interpolation needs a 3-D type-2 plan with kernel width 4..7");
+    p->st = kind == HB_INTERP_STAGED;
+    return HB_OK;
+}
+
 int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s) {
     HB_REQUIRE(p->type == 2, HB_ERR_INVALID_ARG, "coordinate gradient needs a type-2 plan");
     HB_REQUIRE(p->pts_set, HB_ERR_STATE, "coordinate gradient called before setpts");
@@ -1653,6 +1685,9 @@ void plan_free(NufftPlan* p) {
     }
     if (p->dense_parts) cudaFree(p->dense_parts);
     if (p->dense_scratch) cudaFree(p->dense_scratch);
+    if (p->st_jobs) cudaFree(p->st_jobs);
+    p->st_jobs = nullptr;
+    p->n_st_jobs = p->st_cap = 0;
     p->dense_parts = nullptr;
     p->dense_scratch = nullptr;
     p->parts_cap = 0;

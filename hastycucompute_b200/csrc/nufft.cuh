@@ -81,6 +81,12 @@ struct NufftPlan {
     int64_t n_parts = 0, parts_cap = 0;
     float2* dense_scratch = nullptr;
     size_t scratch_cap = 0;  // bytes
+    // staged interpolation (k_interp_st, 3-D, widths 4..7): usable for this plan (st_ok), chosen
+    // (st); the jobs of the current points ({tile, first sorted point, end, 0}), built at setpts
+    bool st_ok = false;
+    bool st = false;
+    int4* st_jobs = nullptr;
+    int64_t n_st_jobs = 0, st_cap = 0;
     size_t device_bytes = 0;
 };
 
@@ -115,6 +121,15 @@ int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* g
 int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx);
 int plan_set_spread_kernel(NufftPlan* p, int kind, int transforms_per_cta);
 int plan_set_interp_tuning(NufftPlan* p, int transforms_per_group);
+int plan_set_interp_kernel(NufftPlan* p, int kind);
+
+// Type-2 interpolation from staged regions of the fine grid (interp_st.cu). interp_st_jobs with
+// jobs == nullptr counts the jobs (per tile in cnt, offsets in off, total in *n_jobs; syncs s);
+// with a job array of jobs_cap >= *n_jobs entries it fills them.
+int interp_st_max_points(int w);
+int interp_st_jobs(const int* bin_start, int64_t ntiles, int w, int* cnt, int* off, int* sums, int4* jobs, int* n_jobs,
+                   int64_t jobs_cap, cudaStream_t s);
+int interp_st_run(const NufftPlan* p, const GridArgs& a, cudaStream_t s);
 void plan_free(NufftPlan* p);
 
 // Pieces reused by the Toeplitz kernel builder.

@@ -7,13 +7,12 @@
 // group (groups take consecutive y rows).
 //
 // Candidate points (the tile's bin and its lower neighbours) pass through shared memory in
-// double-buffered chunks: per point the CC values (cp.async), the tile-relative z and y weights
-// (zero outside the footprint, so a row outside it multiplies by 0 and no row needs a branch)
-// and the raw x taps. A warp visits only the points whose footprint meets its block (one ballot
-// per 32 candidates). For a visited point every lane forms its 4 row products u_r = w_z w_y v and
-// adds w_x[x - x0] u_r to exactly the cells the footprint covers along x: the point's x offset is
-// the same for the whole warp, so a switch over it selects code whose cell range and tap indices
-// are compile-time constants.
+// double-buffered chunks: per point the CC values (cp.async) and its tile-relative weight rows
+// along z, y and x (the kernel taps at the cells the footprint covers, zero elsewhere), so a
+// visit multiplies whole rows with no per-cell range or index logic. A warp visits only the points
+// whose footprint meets its block (ballots per 32 candidates, one per half of the block's 8 x
+// cells). For a visited point every lane forms its 4 row products u_r = w_z w_y v and adds
+// w_x[x] u_r to the 4 x 4 cells of each half of the block that the footprint touches.
 //
 // Dense tiles (more candidates than a subproblem holds, maxp) are spread in ceil(total / maxp)
 // parts, one CTA each, however many that is, so the k-space centre of radial and spiral
@@ -31,8 +30,6 @@
 
 namespace hb {
 
-constexpr int kLcRec = 32;     // weight floats per staged point: wz_t[8] | wy_t[16] | wx[8]
-
 template <int CC, bool D3>
 struct LcShape {
     static constexpr int G = 32 / CC;  // lane groups per warp
@@ -43,50 +40,68 @@ struct LcShape {
     static constexpr int WARPS = NZB * NYB * NXS;
     static constexpr int THREADS = WARPS * 32;
     static constexpr int CELLS = T0 * T1 * T2;
-    // candidates staged per chunk: the 32-transform CTA is alone on its SM (registers), so it
-    // takes long chunks (fewer barriers, even warp loads); smaller CTAs keep several per SM
-    static constexpr int kLcChunk = CC == 32 ? 256 : 128;
-    // staging buffer: values float2[chunk][CC] | weights float[chunk][kLcRec] | packed first cells
+    // weight floats per staged point: tile-relative rows wz[T0] (3-D) | wy[T1] | wx[T2]
+    static constexpr int OY = D3 ? T0 : 0, OX = OY + T1;
+    static constexpr int kRec = OX + T2;
+    // candidates staged per chunk: the 32-transform 3-D CTA is alone on its SM (registers), so it
+    // takes long chunks (fewer barriers, even warp loads); the others keep several per SM
+    static constexpr int kLcChunk = (CC == 32 && D3) ? 256 : 128;
+    // staging buffer: values float2[chunk][CC] | weights float[chunk][kRec] | packed first cells
     static constexpr int kValF = kLcChunk * CC * 2;
-    static constexpr int kBufF = kValF + kLcChunk * kLcRec + kLcChunk;
+    static constexpr int kBufF = kValF + kLcChunk * kRec + kLcChunk;
     static size_t smem_bytes() { return sizeof(float) * (size_t)(kCoefFloats + 2 * kBufF); }
 };
+static_assert(LcShape<32, true>::kRec % 4 == 0 && LcShape<32, false>::kRec % 4 == 0, "16-byte weight rows");
 static_assert(LcShape<32, true>::THREADS == 512 && LcShape<8, true>::THREADS == 128, "tile shape");
 static_assert(LcShape<32, false>::THREADS == 512 && LcShape<8, false>::THREADS == 128, "tile shape");
 
-// acc[r][x] += wx[x - RX] * u_r over the cells x in [0, 8) that the footprint [RX, RX + W) covers
-template <int W, int RX>
-__device__ __forceinline__ void lc_rows(float (&ar)[4][8], float (&ai)[4][8], const float (&wx)[8], const float (&ur)[4],
+// acc[r][X0 + x] += wx[x] * u_r, x < 4
+template <int X0>
+__device__ __forceinline__ void lc_half(float (&ar)[4][8], float (&ai)[4][8], const float4 wx, const float (&ur)[4],
                                         const float (&ui)[4]) {
-    constexpr int lo = RX < 0 ? 0 : RX;
-    constexpr int hi = (RX + W - 1) > 7 ? 7 : (RX + W - 1);
+    const float w[4] = {wx.x, wx.y, wx.z, wx.w};
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
 #pragma unroll
-        for (int x = lo; x <= hi; ++x) {
-            ar[r][x] = fmaf(wx[x - RX], ur[r], ar[r][x]);
-            ai[r][x] = fmaf(wx[x - RX], ui[r], ai[r][x]);
+        for (int x = 0; x < 4; ++x) {
+            ar[r][X0 + x] = fmaf(w[x], ur[r], ar[r][X0 + x]);
+            ai[r][X0 + x] = fmaf(w[x], ui[r], ai[r][X0 + x]);
         }
     }
 }
 
-#define HB_LC_CASE(K)                                                                 \
-    case K:                                                                           \
-        if constexpr ((K) < 8 + W - 1) lc_rows<W, (K) - (W - 1)>(ar, ai, wx, ur, ui); \
-        break;
-
-template <int W>
-__device__ __forceinline__ void lc_dispatch(int k, float (&ar)[4][8], float (&ai)[4][8], const float (&wx)[8],
-                                            const float (&ur)[4], const float (&ui)[4]) {
-    static_assert(W >= 2 && W <= 8, "lanes-on-transforms spreading takes widths 2..8");
-    switch (k) {
-        HB_LC_CASE(0) HB_LC_CASE(1) HB_LC_CASE(2) HB_LC_CASE(3) HB_LC_CASE(4)
-        HB_LC_CASE(5) HB_LC_CASE(6) HB_LC_CASE(7) HB_LC_CASE(8) HB_LC_CASE(9)
-        HB_LC_CASE(10) HB_LC_CASE(11) HB_LC_CASE(12) HB_LC_CASE(13) HB_LC_CASE(14)
-        default: break;
+// A visit's operands: the row products u_r = w_z w_y v of staged point q for this lane's transform
+// and rows, and the x weights of the warp's two halves of 4 cells
+template <int CC, bool D3>
+__device__ __forceinline__ void lc_prep(const float2* bval, const float* bwt, int q, int coil, int z0, int y0g, int x0,
+                                        float (&ur)[4], float (&ui)[4], float4& x0w, float4& x1w) {
+    using S = LcShape<CC, D3>;
+    const float2 v = bval[q * CC + coil];
+    const float* rec = bwt + q * S::kRec;
+    float rw[4];
+    if constexpr (D3) {
+        const float2 wz2 = *reinterpret_cast<const float2*>(rec + z0);
+        const float2 wy2 = *reinterpret_cast<const float2*>(rec + S::OY + y0g);
+        rw[0] = wz2.x * wy2.x;
+        rw[1] = wz2.x * wy2.y;
+        rw[2] = wz2.y * wy2.x;
+        rw[3] = wz2.y * wy2.y;
+    } else {
+        const float4 wy4 = *reinterpret_cast<const float4*>(rec + S::OY + y0g);
+        rw[0] = wy4.x;
+        rw[1] = wy4.y;
+        rw[2] = wy4.z;
+        rw[3] = wy4.w;
     }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        ur[r] = rw[r] * v.x;
+        ui[r] = rw[r] * v.y;
+    }
+    const float4* wx = reinterpret_cast<const float4*>(rec + S::OX + x0);
+    x0w = wx[0];
+    x1w = wx[1];
 }
-#undef HB_LC_CASE
 
 // parts == nullptr: one CTA per tile (blockIdx.x), storing the tile; tiles with more than maxp
 // candidates are left to the parts launch. Otherwise CTA blockIdx.x spreads part e.y of e.z of
@@ -189,7 +204,7 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
         const int n = min(S::kLcChunk, k_end - base);
         float2* bval = reinterpret_cast<float2*>(buf);
         float* bwt = buf + S::kValF;
-        unsigned char* brel = reinterpret_cast<unsigned char*>(bwt + S::kLcChunk * kLcRec);
+        unsigned char* brel = reinterpret_cast<unsigned char*>(bwt + S::kLcChunk * S::kRec);
         constexpr int CP = CC / 2;               // 16-byte pieces of a point's values
         constexpr int PPA = (CP + 2) / 3;        // pieces per axis thread
         for (int i = tid; i < 3 * n; i += S::THREADS) {
@@ -216,31 +231,22 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
                 *reinterpret_cast<int*>(brel + q * 4) =
                     reach ? (rel[0] + 16) | ((rel[1] + 16) << 8) | ((rel[2] + 16) << 16) : 0;
             if (!reach) continue;
-            float* rec = bwt + q * kLcRec;
-            if (ax == 0 && !D3) {
-                reinterpret_cast<float4*>(rec)[0] = make_float4(1.f, 0.f, 0.f, 0.f);
-                reinterpret_cast<float4*>(rec)[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
+            if (D3 || ax != 0) {
+                // this axis's tile-relative weight row: the W taps at cells rel .. rel+W-1 inside
+                // the tile, zero elsewhere
                 const float v = __fsub_rn(a.su[ax][sidx], hw);
                 const float sarg = fmaf(2.f, __fsub_rn(ceilf(v), v), -1.f);
                 float t[W];
 #pragma unroll
                 for (int d = 0; d < W; ++d) t[d] = kb_tap(coef, a.kb.deg, d, sarg);
-                if (ax == 2) {
-                    reinterpret_cast<float4*>(rec + 24)[0] = make_float4(t[0], t[1], t[2], t[3]);
-                    reinterpret_cast<float4*>(rec + 24)[1] =
-                        make_float4(W > 4 ? t[4 % W] : 0.f, W > 5 ? t[5 % W] : 0.f, W > 6 ? t[6 % W] : 0.f,
-                                    W > 7 ? t[7 % W] : 0.f);
-                } else {
-                    const int T = ax == 0 ? S::T0 : S::T1;
-                    float* wt = rec + (ax == 0 ? 0 : 8);
-                    const int r = ax == 0 ? rel[0] : rel[1];
-                    for (int c = 0; c < T; c += 4) *reinterpret_cast<float4*>(wt + c) = make_float4(0.f, 0.f, 0.f, 0.f);
+                const int T = ax == 0 ? S::T0 : (ax == 1 ? S::T1 : S::T2);
+                float* wt = bwt + q * S::kRec + (ax == 0 ? 0 : (ax == 1 ? S::OY : S::OX));
+                const int r = ax == 0 ? rel[0] : (ax == 1 ? rel[1] : rel[2]);
+                for (int c = 0; c < T; c += 4) *reinterpret_cast<float4*>(wt + c) = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-                    for (int d = 0; d < W; ++d) {
-                        const int c = r + d;
-                        if (c >= 0 && c < T) wt[c] = t[d];
-                    }
+                for (int d = 0; d < W; ++d) {
+                    const int c = r + d;
+                    if (c >= 0 && c < T) wt[c] = t[d];
                 }
             }
             const float2* src = a.inT + (int64_t)a.perm[sidx] * g.C;
@@ -278,49 +284,38 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
                 const float* buf = region + (it & 1) * S::kBufF;
                 const float2* bval = reinterpret_cast<const float2*>(buf);
                 const float* bwt = buf + S::kValF;
-                const int* brel = reinterpret_cast<const int*>(bwt + S::kLcChunk * kLcRec);
+                const int* brel = reinterpret_cast<const int*>(bwt + S::kLcChunk * S::kRec);
                 for (int q0 = 0; q0 < n; q0 += 32) {
                     const int qq = q0 + lane;
-                    bool hit = false;
+                    bool h0 = false, h1 = false;
                     if (qq < n) {
                         const int pk = brel[qq];
                         const int rz = (pk & 0xff) - 16, ry = ((pk >> 8) & 0xff) - 16, rx = ((pk >> 16) & 0xff) - 16;
-                        hit = rz <= z0 + S::RZ - 1 && rz + WZ - 1 >= z0 && ry <= y0w + S::G * S::RY - 1 &&
-                              ry + W - 1 >= y0w && rx <= x0 + 7 && rx + W - 1 >= x0;
+                        const bool zy = rz <= z0 + S::RZ - 1 && rz + WZ - 1 >= z0 && ry <= y0w + S::G * S::RY - 1 &&
+                                        ry + W - 1 >= y0w;
+                        h0 = zy && rx <= x0 + 3 && rx + W - 1 >= x0;
+                        h1 = zy && rx <= x0 + 7 && rx + W - 1 >= x0 + 4;
                     }
-                    unsigned bits = __ballot_sync(0xffffffffu, hit);
+                    const unsigned m0 = __ballot_sync(0xffffffffu, h0), m1 = __ballot_sync(0xffffffffu, h1);
+                    unsigned bits = m0 | m1;
+                    // visits two at a time: both points' loads and row products are issued before
+                    // either's multiply-adds, so one visit's shared-memory latency hides behind the
+                    // other's arithmetic
                     while (bits) {
-                        const int q = q0 + __ffs(bits) - 1;
+                        const int ia = __ffs(bits) - 1;
                         bits &= bits - 1;
-                        const int k = ((brel[q] >> 16) & 0xff) - 16 - x0 + (W - 1);
-                        const float2 v = bval[q * CC + coil];
-                        const float* rec = bwt + q * kLcRec;
-                        float rw[4];
-                        if constexpr (D3) {
-                            const float2 wz2 = *reinterpret_cast<const float2*>(rec + z0);
-                            const float2 wy2 = *reinterpret_cast<const float2*>(rec + 8 + y0g);
-                            rw[0] = wz2.x * wy2.x;
-                            rw[1] = wz2.x * wy2.y;
-                            rw[2] = wz2.y * wy2.x;
-                            rw[3] = wz2.y * wy2.y;
-                        } else {
-                            const float4 wy4 = *reinterpret_cast<const float4*>(rec + 8 + y0g);
-                            rw[0] = wy4.x;
-                            rw[1] = wy4.y;
-                            rw[2] = wy4.z;
-                            rw[3] = wy4.w;
-                        }
-                        float ur[4], ui[4];
-#pragma unroll
-                        for (int r = 0; r < 4; ++r) {
-                            ur[r] = rw[r] * v.x;
-                            ui[r] = rw[r] * v.y;
-                        }
-                        {
-                            const float4 xa = *reinterpret_cast<const float4*>(rec + 24);
-                            const float4 xb = *reinterpret_cast<const float4*>(rec + 28);
-                            const float wx[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-                            lc_dispatch<W>(k, ar, ai, wx, ur, ui);
+                        const bool two = bits != 0;
+                        const int ib = two ? __ffs(bits) - 1 : ia;
+                        if (two) bits &= bits - 1;
+                        float ura[4], uia[4], urb[4], uib[4];
+                        float4 xa0, xa1, xb0, xb1;
+                        lc_prep<CC, D3>(bval, bwt, q0 + ia, coil, z0, y0g, x0, ura, uia, xa0, xa1);
+                        lc_prep<CC, D3>(bval, bwt, q0 + ib, coil, z0, y0g, x0, urb, uib, xb0, xb1);
+                        if ((m0 >> ia) & 1u) lc_half<0>(ar, ai, xa0, ura, uia);
+                        if ((m1 >> ia) & 1u) lc_half<4>(ar, ai, xa1, ura, uia);
+                        if (two) {
+                            if ((m0 >> ib) & 1u) lc_half<0>(ar, ai, xb0, urb, uib);
+                            if ((m1 >> ib) & 1u) lc_half<4>(ar, ai, xb1, urb, uib);
                         }
                     }
                 }

@@ -176,6 +176,15 @@ class NufftPlan:
         automatic). All choices compute the same sums."""
         _lib.call("hb_nufft_set_interp_tuning", self._h, int(transforms_per_group))
 
+    def set_interp_kernel(self, kind: str = "auto") -> None:
+        """Interpolation (type 2): "gather" (each point's cells from global memory), "staged" (per
+        8^3 tile and 8 transforms, the reachable region copied to shared memory first; 3-D, widths
+        4..7) or "auto". Both give bit-identical samples."""
+        kinds = {"auto": 0, "gather": 1, "staged": 2}
+        if kind not in kinds:
+            raise ValueError(f"interpolation kernel must be one of {sorted(kinds)}")
+        _lib.call("hb_nufft_set_interp_kernel", self._h, kinds[kind])
+
     def info(self) -> PlanInfo:
         fine = (C.c_int64 * 3)()
         w = C.c_int()

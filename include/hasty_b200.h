@@ -122,6 +122,16 @@ int hb_nufft_set_spread_kernel(hb_nufft_plan plan, int kind, int transforms_per_
  * warp in flight at once. Every choice computes the same sums. */
 int hb_nufft_set_interp_tuning(hb_nufft_plan plan, int transforms_per_group);
 
+/* Interpolation kernel of a type-2 plan (no counterpart in the reference): HB_INTERP_GATHER
+ * (warps gather each point's cells from global memory, any plan), HB_INTERP_STAGED (one CTA per
+ * 8^3 tile and 8 transforms copies the region the tile's footprints reach into shared memory and
+ * gathers from there; 3-D plans with kernel width 4..7, else HB_ERR_INVALID_ARG) or HB_INTERP_AUTO.
+ * Both kernels give bit-identical samples; callable before or after setpts. */
+#define HB_INTERP_AUTO   0
+#define HB_INTERP_GATHER 1
+#define HB_INTERP_STAGED 2
+int hb_nufft_set_interp_kernel(hb_nufft_plan plan, int kind);
+
 /* Coordinate gradient (no counterpart in the reference, which has no derivatives): with a
  * type-2 plan (sign s) whose points are set, writes to grad ([dim][M] float, image order)
  *   grad[i][j] = -(nf_i / 2 pi) Re( sum_c h[c][j] sum_l G_c[l] dPhi_i(l - u_j) )

@@ -66,3 +66,26 @@ def test_transforms_on_lanes_is_refused_where_the_plan_does_not_allow_it(cuda):
     with pytest.raises(hb.HastyError, match="INVALID_ARG"):
         p.set_spread_kernel("transforms")
     p.set_spread_kernel("cells")
+
+
+@pytest.mark.gpu
+def test_interp_tuner_picks_caches_and_applies(cuda, tmp_path, monkeypatch):
+    """Type-2 lane-group tuning: every size is timed, the choice is cached, and a plan given it
+    interpolates the oracle's samples."""
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200 import autotune
+    monkeypatch.setenv("HASTY_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    rng = np.random.default_rng(4)
+    nmodes, T, w, M = (40, 48), 12, 4, 20000
+    coords = rand_coords(rng, 2, M)
+    dcoords = [to_dev(x, cuda) for x in coords]
+    first = autotune.tune_interp(nmodes, T, dcoords, w)
+    assert not first["cached"] and first["interp_group"] in autotune.INTERP_GROUPS
+    assert sorted(g for _, g in first["timings"]) == sorted(autotune.INTERP_GROUPS)
+    again = autotune.tune_interp(nmodes, T, dcoords, w)
+    assert again["cached"] and again["interp_group"] == first["interp_group"]
+    f = crand(rng, T, *nmodes)
+    p = hb.NufftPlan(hb.NufftType.TYPE_2, hb.NufftOpts(nmodes=nmodes, ntransf=T, kernel_width=w))
+    autotune.apply(p, first)
+    p.setpts(dcoords)
+    assert relerr(to_np(p(to_dev(f, cuda))), gridding.nufft2(coords, f, w=w)) <= 1e-5
