@@ -418,6 +418,7 @@ def bench_nufft(args, hb, _lib, coords, wl, dev, stream, hbm_peak):
     shape, C, M, w = wl["shape"], wl["C"], wl["M"], wl["w"]
     opts = hb.NufftOpts(nmodes=shape, ntransf=C, kernel_width=w)
     p2 = hb.NufftPlan(hb.NufftType.TYPE_2, opts)
+    p2.set_interp_kernel(args.interp_kernel)
     p2.setpts(coords)
     f = torch.from_numpy(wl["smaps"]).to(dev) * torch.from_numpy(wl["x"]).to(dev)[None]
     y = torch.empty((C, M), dtype=torch.complex64, device=dev)
@@ -834,6 +835,8 @@ def main(argv=None):
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--interp-kernel", choices=["auto", "gather", "staged"], default="auto",
+                    help="type-2 interpolation kernel of the NUFFT leg (both give bit-identical samples)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
