@@ -9,9 +9,10 @@
 //
 // Bank layout: a cell is 8 transforms x 8 B = 64 B, half of the 128-byte bank window, and the
 // region's row pitches are odd, so a cell's half of the banks is the parity of z + y + x. Every tap
-// of a point keeps the parity of its first cell, so a warp whose four lane groups hold two points
-// of each parity reads two cells per half per load: the minimum two wavefronts. The CTA orders its
-// points into such quadruples (even, even, odd, odd) and runs the unmatched rest after them.
+// of a point keeps the parity of its first cell. An 8-byte load is served per half-warp (two lane
+// groups), so a half-warp whose two groups hold points of opposite parity reads its two cells in
+// one wavefront: the minimum two per warp load. The CTA orders its points into such quadruples
+// (even, odd, even, odd) and runs the unmatched rest after them.
 //
 // The sums run in the order of the gathering kernel (per row the x taps, then the row weight
 // w_z w_y), with the same tap weights, so both kernels give bit-identical samples.
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
         if (ax == 0) pidx[q] = a.perm[sidx];
     }
     __syncthreads();
-    // parity classes, then the visit order: quadruples (even, even, odd, odd), then the rest
+    // parity classes, then the visit order: quadruples (even, odd, even, odd), then the rest
     for (int q = tid; q < n; q += kStThreads) {
         const int pk = rel[q];
         const int par = ((pk & 0xff) + ((pk >> 8) & 0xff) + ((pk >> 16) & 0xff)) & 1;
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
         __syncthreads();
         if (tid < n) {
             const int par = o >> 30, i = o & 0x3fffffff;
-            const int slot = i < 2 * m2 ? 4 * (i >> 1) + 2 * par + (i & 1)
+            const int slot = i < 2 * m2 ? 4 * (i >> 1) + 2 * (i & 1) + par
                                         : 4 * m2 + (par ? ne - 2 * m2 : 0) + (i - 2 * m2);
             order[slot] = tid;
         }

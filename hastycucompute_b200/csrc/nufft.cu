@@ -1183,6 +1183,24 @@ static int auto_subproblem(int64_t M, const GridGeom& g) {
     return m;
 }
 
+// Job list of the staged interpolation kernel for the current points (type-2 plans).
+static int st_build_jobs(NufftPlan* p, cudaStream_t s) {
+    int n_jobs = 0;
+    HB_TRY(interp_st_jobs(p->bin_start, p->nbins, p->g.wa[2], p->tmp_ecnt, p->tmp_eoff, p->tmp_sums, nullptr, &n_jobs, 0, s));
+    if (n_jobs > p->st_cap) {
+        if (p->st_jobs) cudaFree(p->st_jobs);
+        p->st_jobs = nullptr;
+        p->st_cap = 0;
+        HB_TRY(dev_alloc(p, (void**)&p->st_jobs, sizeof(int4) * n_jobs, "staged interpolation jobs"));
+        p->st_cap = n_jobs;
+    }
+    HB_TRY(interp_st_jobs(p->bin_start, p->nbins, p->g.wa[2], p->tmp_ecnt, p->tmp_eoff, p->tmp_sums, p->st_jobs, &n_jobs,
+                          p->st_cap, s));
+    p->n_st_jobs = n_jobs;
+    p->st_built = true;
+    return HB_OK;
+}
+
 int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const float* c2, cudaStream_t s) {
     GridGeom& g = p->g;
     HB_REQUIRE(M >= 0 && M < (int64_t)0x7fffffff, HB_ERR_INVALID_ARG, "M must be in [0, 2^31)");
@@ -1341,24 +1359,8 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
                 if ((st = check_launch("k_tile_extra_fill")) != HB_OK) break;
             }
         }
-        if (p->type == 2 && p->st_ok) {
-            int n_jobs = 0;
-            if ((st = interp_st_jobs(p->bin_start, p->nbins, g.wa[2], ecnt, eoff, p->tmp_sums, nullptr, &n_jobs, 0, s)) !=
-                HB_OK)
-                break;
-            if (n_jobs > p->st_cap) {
-                if (p->st_jobs) cudaFree(p->st_jobs);
-                p->st_jobs = nullptr;
-                p->st_cap = 0;
-                if ((st = dev_alloc(p, (void**)&p->st_jobs, sizeof(int4) * n_jobs, "staged interpolation jobs")) != HB_OK)
-                    break;
-                p->st_cap = n_jobs;
-            }
-            if ((st = interp_st_jobs(p->bin_start, p->nbins, g.wa[2], ecnt, eoff, p->tmp_sums, p->st_jobs, &n_jobs,
-                                     p->st_cap, s)) != HB_OK)
-                break;
-            p->n_st_jobs = n_jobs;
-        }
+        p->st_built = false;
+        if (p->type == 2 && p->st && (st = st_build_jobs(p, s)) != HB_OK) break;
         {
             int err = 0;
             if ((e = cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
@@ -1641,6 +1643,11 @@ int plan_set_interp_kernel(NufftPlan* p, int kind) {
     HB_REQUIRE(kind != HB_INTERP_STAGED || p->st_ok, HB_ERR_INVALID_ARG,
                "staged interpolation needs a 3-D type-2 plan with kernel width 4..7");
     p->st = kind == HB_INTERP_STAGED;
+    // points already set: build the staged kernel's job list now (setpts builds it otherwise)
+    if (p->st && p->pts_set && !p->st_built) {
+        HB_TRY(st_build_jobs(p, nullptr));
+        HB_CUDA(cudaStreamSynchronize(nullptr));
+    }
     return HB_OK;
 }
 

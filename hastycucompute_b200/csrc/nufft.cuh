@@ -85,6 +85,7 @@ struct NufftPlan {
     // (st); the jobs of the current points ({tile, first sorted point, end, 0}), built at setpts
     bool st_ok = false;
     bool st = false;
+    bool st_built = false;  // st_jobs match the current points
     int4* st_jobs = nullptr;
     int64_t n_st_jobs = 0, st_cap = 0;
     size_t device_bytes = 0;

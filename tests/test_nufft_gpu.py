@@ -305,12 +305,17 @@ def test_staged_interp_matches_gather_and_oracle(cuda, nmodes, T, w):
         coords.append(np.clip(x, -np.pi, np.pi - 1e-6).astype(np.float32))
     f = crand(rng, T, *nmodes)
     outs = {}
-    for kernel in ("gather", "staged"):
+    for kernel, after in (("gather", False), ("staged", False), ("staged", True)):
         p = hb.NufftPlan(hb.NufftType.TYPE_2, hb.NufftOpts(nmodes=nmodes, ntransf=T, kernel_width=w))
-        p.set_interp_kernel(kernel)
+        if not after:
+            p.set_interp_kernel(kernel)
         p.setpts([to_dev(x, cuda) for x in coords])
-        outs[kernel] = to_np(p(to_dev(f, cuda)))
-    assert np.array_equal(outs["staged"], outs["gather"])
+        if after:  # chosen once the points are set: the job list is built then
+            p.set_interp_kernel(kernel)
+        outs[(kernel, after)] = to_np(p(to_dev(f, cuda)))
+    assert np.array_equal(outs[("staged", False)], outs[("gather", False)])
+    assert np.array_equal(outs[("staged", True)], outs[("gather", False)])
+    outs["staged"] = outs[("staged", False)]
     assert relerr(outs["staged"], gridding.nufft2(coords, f, w=w)) <= 1e-5
 
 
