@@ -134,6 +134,11 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// waits until at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // Op::kStageRow (optional, default false): on zero-padded inputs each sample is
 // load_col(a, l, e) * row(a, e0)[l] when row_shared(e0, E_blk) (one row factor for all columns
@@ -146,6 +151,26 @@ template <class Op>
 struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
     static constexpr bool value = Op::kStageRow;
 };
+
+// Op::kPrefetch (optional, default false; zero-padded inputs, Lin == L/2 at shift 0): the CTAs are
+// persistent and walk the column blocks with a stride of the grid; each block's samples arrive in
+// shared memory by cp.async issued while the previous block is transformed, and Op::src(l, e)
+// gives the sample's address (columns contiguous along e).
+template <class Op, class = void>
+struct Prefetch {
+    static constexpr bool value = false;
+};
+template <class Op>
+struct Prefetch<Op, std::void_t<decltype(Op::kPrefetch)>> {
+    static constexpr bool value = Op::kPrefetch;
+};
+
+// kernel columns a fused CTA stages: two for the prefetching passes (which also hold a block of
+// samples and must keep three CTAs per SM), kMaxKCols otherwise
+template <class Op>
+constexpr int max_kcols() {
+    return Prefetch<Op>::value ? 2 : kMaxKCols;
+}
 
 // Op contract (in addition to fft.cuh's):
 //   static constexpr bool kStoreLFast    // destination contiguous along the output index
@@ -168,15 +193,17 @@ struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
 // from the pass's lengths and shifts.
 //
 // CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (95 registers; at 64 it spills
-// and runs slower), the fused-kernel pass 3 (64 registers; at 2 CTAs it runs slower), every other
-// pass 4 (48 registers, a few spilled words): they move bytes, and the fourth CTA hides more of
-// the load latency than the spills cost.
-template <class Op>
+// and runs slower), the prefetching fused-kernel pass at L = 320 2 (96 registers: its samples
+// arrive by cp.async while the previous block is transformed; at 3 CTAs, 64 registers, it spills
+// 328 bytes per thread and runs 22 % slower), other fused-kernel passes 3, every other pass 4 (48
+// registers, a few spilled words): they move bytes, and the fourth CTA hides more of the load
+// latency than the spills cost.
+template <class Op, int L>
 constexpr int pass2_min_blocks() {
-    return Op::kSenseReduce ? 2 : Op::kFusedK ? 3 : 4;
+    return Op::kSenseReduce ? 2 : (Op::kFusedK ? ((Prefetch<Op>::value && L == 320) ? 2 : 3) : 4);
 }
 template <int P, int Q, class Op, int HM = 0>
-__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks<Op>()) pass2_kernel(const Op op, const PassCfg c) {
+__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks<Op, P * Q>()) pass2_kernel(const Op op, const PassCfg c) {
     constexpr int L = P * Q;
     constexpr int CWp = kCW + 1;
     constexpr bool kHalfIn = (HM & 1) != 0;
@@ -197,9 +224,12 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
     float2* T2 = tw + L;               // kT2: [Q][P], T2[t * P + k1] = W_L^(t k1)
     float2* Y = T2 + (kT2 ? L : 0);    // [L][CWp] transpose buffer
     float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][groups][Lout] running sums
-    float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * op.ngroups() * c.Lout : 0);  // kFusedK: [kMaxKCols][L]
-    float2* Ss = Ks + (Op::kFusedK ? kMaxKCols * L : 0);          // kSenseReduce: [W][Lout]
+    constexpr bool kPf = Prefetch<Op>::value;
+    static_assert(!kPf || (kHalfIn && Op::kFusedK && !StageRow<Op>::value), "prefetch: fused passes on padded inputs");
+    float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * op.ngroups() * c.Lout : 0);  // kFusedK: [max_kcols][L]
+    float2* Ss = Ks + (Op::kFusedK ? max_kcols<Op>() * L : 0);    // kSenseReduce: [W][Lout]
     float2* Rs = Ss + (Op::kSenseReduce ? c.W * c.Lout : 0);      // StageRow: [A_blk][L/2]
+    float2* Pf = Rs + (StageRow<Op>::value ? c.A_blk * (L / 2) : 0);  // kPf: [L/2][kCW] samples
 
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
         tw[i] = c.tw[i];
@@ -210,8 +240,14 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
     const int out_shift = ((c.out_shift % L) + L) % L;
     __syncthreads();
 
-    int64_t ab, eb_begin, eb_end;
-    if (Op::kChunkLoop) {
+    int64_t ab, eb_begin, eb_end, eb_step = 1;
+    if (kPf) {
+        // one outer row (A == 1, A_blk == 1: checked by the launcher); blocks blockIdx.x, +gridDim.x, ...
+        ab = 0;
+        eb_begin = blockIdx.x;
+        eb_end = c.n_eb;
+        eb_step = gridDim.x;
+    } else if (Op::kChunkLoop) {
         ab = blockIdx.x;
         eb_begin = 0;
         eb_end = c.n_eb;
@@ -221,6 +257,29 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
         eb_end = eb_begin + 1;
     }
     const int64_t a0 = ab * c.A_blk;
+    // kPf: the samples l < L/2 of block eb's kCW columns into Pf[l][col] (16-byte copies of two
+    // columns where both exist and are aligned, else one column at a time; missing columns are 0)
+    auto prefetch = [&](int64_t eb) {
+        if constexpr (kPf) {
+            const int64_t e0p = eb * c.E_blk;
+            constexpr int PC = kCW / 2;
+#pragma unroll 1
+            for (int i = tid; i < (L / 2) * PC; i += blockDim.x) {
+                const int l = i / PC, pc = i - l * PC;
+                const int64_t e = e0p + 2 * pc;
+                float2* dst = Pf + l * kCW + 2 * pc;
+                const float2* src = op.src(l, e);
+                if (e + 1 < c.E && ((uintptr_t)src & 15) == 0) {
+                    cp_async16(dst, src);
+                } else {
+                    if (e < c.E) cp_async8(dst, src); else dst[0] = make_float2(0.f, 0.f);
+                    if (e + 1 < c.E) cp_async8(dst + 1, src + 1); else dst[1] = make_float2(0.f, 0.f);
+                }
+            }
+            cp_async_commit();
+        }
+    };
+    if (kPf && eb_begin < eb_end) prefetch(eb_begin);
     // column -> (row in the block, inner index); with one row per CTA (every large problem) the
     // runtime division by E_blk is skipped
     auto split_col = [&](int col, int& al, int& el) {
@@ -237,7 +296,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
         __syncthreads();
     }
 
-    for (int64_t eb = eb_begin; eb < eb_end; ++eb) {
+    for (int64_t eb = eb_begin; eb < eb_end; eb += eb_step) {
         const int64_t e0 = eb * c.E_blk;
         // ---- stage the kernel columns / factor rows this chunk needs (asynchronous) -----------
         int64_t kc0 = 0;
@@ -247,11 +306,16 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
             const int64_t elast = min(e0 + c.E_blk, c.E) - 1;
             kc0 = op.kcol(e0);
             nk = (int)(op.kcol(elast) - kc0 + 1);
-            k_staged = (c.A_blk == 1) && nk <= kMaxKCols;
+            k_staged = (c.A_blk == 1) && nk <= max_kcols<Op>();
             if (k_staged) {
                 for (int i = tid; i < nk * L; i += blockDim.x) cp_async8(Ks + i, op.kptr(kc0 + i / L) + (i % L));
                 cp_async_commit();
             }
+        }
+        if constexpr (kPf) {
+            // this block's samples (the group before the kernel columns just issued)
+            if (k_staged) cp_async_wait_group<1>(); else cp_async_wait_all();
+            __syncthreads();
         }
         if constexpr (Op::kSenseReduce) {
             // one warp per column row: the row pointer once, then contiguous copies
@@ -316,6 +380,10 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                         if (colok) v[j] = cmul(v[j], op.row_at(a, t + Q * j, e));
                 }
                 halfzero = true;
+            } else if constexpr (kHalfIn && kPf) {
+#pragma unroll
+                for (int j = 0; j < P; ++j) v[j] = (j < P / 2) ? Pf[(t + Q * j) * kCW + col] : make_float2(0.f, 0.f);
+                halfzero = true;
             } else if constexpr (kHalfIn) {
 #pragma unroll
                 for (int j = 0; j < P; ++j)
@@ -359,6 +427,8 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
         }
         if (Op::kFusedK || Op::kSenseReduce) cp_async_wait_all();
         __syncthreads();
+        // every thread has read Pf: the next block's samples load while this one is transformed
+        if (kPf && eb + eb_step < eb_end) prefetch(eb + eb_step);
         // ---- step 2: thread (col, k1) runs the Q-point DFT ----------------------------------------
         const bool s2active = tid < P * kCW;
         int col2 = 0, k1 = 0;
@@ -521,7 +591,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 }
             }
         }
-        if (eb + 1 < eb_end) __syncthreads();  // the next chunk rewrites Y (and the staged rows)
+        if (eb + eb_step < eb_end) __syncthreads();  // the next chunk rewrites Y (and the staged rows)
     }
     if constexpr (Op::kSenseReduce) {
         __syncthreads();
@@ -569,8 +639,25 @@ int launch_pass2_inst(const Op& op, const PassCfg& c, size_t smem, int64_t block
         set_error(std::string(name) + ": cudaFuncSetAttribute failed: " + cudaGetErrorString(e));
         return HB_ERR_CUDA;
     }
+    int64_t grid = blocks;
+    if constexpr (Prefetch<Op>::value) {
+        // persistent CTAs: as many as are resident at once
+        static int per_sm = 0, sms = 0;
+        if (per_sm == 0) {
+            int dev = 0, n = 0, m = 0;
+            if (cudaGetDevice(&dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pass2_kernel<P, Q, Op, HM>, Q * kCW, smem) != cudaSuccess) {
+                set_error(std::string(name) + ": occupancy query failed");
+                return HB_ERR_CUDA;
+            }
+            sms = m;
+            per_sm = n > 0 ? n : 1;
+        }
+        grid = std::min<int64_t>(blocks, (int64_t)per_sm * sms);
+    }
     TimedSection ts(name, s);
-    pass2_kernel<P, Q, Op, HM><<<(unsigned)blocks, Q * kCW, smem, s>>>(op, c);
+    pass2_kernel<P, Q, Op, HM><<<(unsigned)grid, Q * kCW, smem, s>>>(op, c);
     return check_launch(name);
 }
 
@@ -589,11 +676,16 @@ int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s,
         }
     }
     size_t smem = (size_t)((Op::kFusedK || !Op::kLoadLFast ? 2 : 1) * L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
-    if (Op::kFusedK) smem += (size_t)kMaxKCols * L * sizeof(float2);
+    if (Op::kFusedK) smem += (size_t)max_kcols<Op>() * L * sizeof(float2);
+    if (Prefetch<Op>::value) smem += (size_t)(L / 2) * kCW * sizeof(float2);
     if (Op::kSenseReduce) smem += (size_t)c.W * c.Lout * sizeof(float2);
     if (StageRow<Op>::value) smem += (size_t)c.A_blk * (L / 2) * sizeof(float2);
     const int64_t n_ab = ceil_div(c.A, c.A_blk);
     const int64_t blocks = Op::kChunkLoop ? n_ab : n_ab * c.n_eb;
+    if (Prefetch<Op>::value && (c.A != 1 || c.A_blk != 1 || (c.E_blk != kCW && c.n_eb != 1))) {
+        set_error(std::string(name) + ": a prefetching pass takes one outer row of kCW-column blocks");
+        return HB_ERR_INVALID_ARG;
+    }
     if (blocks <= 0) return HB_OK;
     if (blocks > 0x7fffffffLL) {
         set_error(std::string(name) + ": grid too large");

@@ -177,6 +177,7 @@ struct OpStridedCrop : OpStrided {
 // In-place fused pass: FFT, * Kt[col][pos], IFFT, crop. buf[l][e] with row stride E.
 struct OpToepMid {
     static constexpr int kHalfIO = 3;  // pass shape (pass2_kernel HM)
+    static constexpr bool kPrefetch = true;  // persistent CTAs, next block's samples by cp.async
     static constexpr bool kLoadLFast = false;
     static constexpr bool kStoreLFast = false;
     static constexpr bool kFusedK = true;
@@ -187,6 +188,7 @@ struct OpToepMid {
     int64_t E, B;
     int Lk;
     __device__ __forceinline__ float2 load(int64_t, int l, int64_t e) const { return buf[(int64_t)l * E + e]; }
+    __device__ __forceinline__ const float2* src(int l, int64_t e) const { return buf + (int64_t)l * E + e; }
     __device__ __forceinline__ int64_t kcol(int64_t e) const { return e / B; }
     __device__ __forceinline__ const float2* kptr(int64_t kc) const { return kt + kc * Lk; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }

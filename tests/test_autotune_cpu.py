@@ -61,3 +61,40 @@ def test_unreadable_cache_counts_as_empty(tmp_path, monkeypatch):
     assert autotune._load() == {}
     monkeypatch.setenv("HASTY_B200_TUNE_CACHE", str(tmp_path / "missing.json"))
     assert autotune._load() == {}
+
+
+def test_interp_choice_is_cached_apart_from_spreading(tmp_path, monkeypatch):
+    """The interpolation tuner keys its choices apart from the spreading tuner's, returns a cached
+    choice without building plans, and apply() sets only what a choice holds."""
+    monkeypatch.setenv("HASTY_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    c = _coords(5000)
+    key = autotune._key((16, 16, 16), 12, 4, c)
+    autotune._store({"interp|" + key: {"interp_group": 4, "ms": 0.1, "timings": []},
+                     key: {"kernel": "cells", "block": [2, 4, 4], "max_candidates": 1024, "ms": 0.2, "timings": []}})
+
+    def no_plans(*a, **k):
+        raise AssertionError("a cached choice must not build plans")
+
+    monkeypatch.setattr(autotune, "NufftPlan", no_plans)
+    got = autotune.tune_interp((16, 16, 16), 12, c, 4)
+    assert got["cached"] is True and got["interp_group"] == 4
+    spread = autotune.tune_spread((16, 16, 16), 12, c, 4)
+    assert spread["cached"] is True and spread["kernel"] == "cells"
+
+    calls = []
+
+    class FakePlan:
+        def set_spread_kernel(self, k):
+            calls.append(("kernel", k))
+
+        def set_spread_tuning(self, m, b):
+            calls.append(("tuning", m, b))
+
+        def set_interp_tuning(self, g):
+            calls.append(("interp", g))
+
+    autotune.apply(FakePlan(), got)
+    assert calls == [("interp", 4)]
+    calls.clear()
+    autotune.apply(FakePlan(), dict(spread, **got))
+    assert calls == [("kernel", "cells"), ("tuning", 1024, (2, 4, 4)), ("interp", 4)]
