@@ -152,10 +152,12 @@ struct StageRow<Op, std::void_t<decltype(Op::kStageRow)>> {
     static constexpr bool value = Op::kStageRow;
 };
 
-// Op::kPrefetch (optional, default false; zero-padded inputs, Lin == L/2 at shift 0): the CTAs are
-// persistent and walk the column blocks with a stride of the grid; each block's samples arrive in
-// shared memory by cp.async issued while the previous block is transformed, and Op::src(l, e)
-// gives the sample's address (columns contiguous along e).
+// Op::kPrefetch (optional, default false; inputs at fixed positions: zero-padded Lin == L/2 or the
+// full L, shift 0): where a CTA holds one outer row (A_blk == 1) the CTAs are persistent and walk
+// the (row, column block) jobs with a stride of the grid (a chunk-looping operator keeps all blocks
+// of a row on one CTA); each job's samples arrive in shared memory by cp.async issued while the
+// previous job is transformed, and Op::sample_ptr(a, l, e) gives the sample's address (columns contiguous
+// along e). Other block shapes run the same operator without prefetching.
 template <class Op, class = void>
 struct Prefetch {
     static constexpr bool value = false;
@@ -166,10 +168,10 @@ struct Prefetch<Op, std::void_t<decltype(Op::kPrefetch)>> {
 };
 
 // kernel columns a fused CTA stages: two for the prefetching passes (which also hold a block of
-// samples and must keep three CTAs per SM), kMaxKCols otherwise
-template <class Op>
+// samples in shared memory), kMaxKCols otherwise
+template <bool PF>
 constexpr int max_kcols() {
-    return Prefetch<Op>::value ? 2 : kMaxKCols;
+    return PF ? 2 : kMaxKCols;
 }
 
 // Op contract (in addition to fft.cuh's):
@@ -193,17 +195,19 @@ constexpr int max_kcols() {
 // from the pass's lengths and shifts.
 //
 // CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (95 registers; at 64 it spills
-// and runs slower), the prefetching fused-kernel pass at L = 320 2 (96 registers: its samples
-// arrive by cp.async while the previous block is transformed; at 3 CTAs, 64 registers, it spills
-// 328 bytes per thread and runs 22 % slower), other fused-kernel passes 3, every other pass 4 (48
+// and runs slower; prefetching the next chunk, 160^3 x 32 coils: 0.875 against 0.957 ms), the
+// prefetching fused-kernel pass at L = 320 2 (96 registers: its samples arrive by cp.async while
+// the previous block is transformed, 3.66 against 4.03 ms; at 3 CTAs, 64 registers, it spills 328
+// bytes per thread and runs 22 % slower), other fused-kernel passes 3, every other pass 4 (48
 // registers, a few spilled words): they move bytes, and the fourth CTA hides more of the load
-// latency than the spills cost.
-template <class Op, int L>
+// latency than the spills cost (prefetching them at 2 or 3 CTAs measured slower).
+template <class Op, int L, int HM, bool PF>
 constexpr int pass2_min_blocks() {
-    return Op::kSenseReduce ? 2 : (Op::kFusedK ? ((Prefetch<Op>::value && L == 320) ? 2 : 3) : 4);
+    return Op::kSenseReduce ? 2 : Op::kFusedK ? ((PF && L == 320) ? 2 : 3) : (PF ? ((HM & 1) ? 3 : 2) : 4);
 }
-template <int P, int Q, class Op, int HM = 0>
-__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks<Op, P * Q>()) pass2_kernel(const Op op, const PassCfg c) {
+template <int P, int Q, class Op, int HM = 0, bool PF = false>
+__global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks<Op, P * Q, HM, PF>())
+    pass2_kernel(const Op op, const PassCfg c) {
     constexpr int L = P * Q;
     constexpr int CWp = kCW + 1;
     constexpr bool kHalfIn = (HM & 1) != 0;
@@ -224,12 +228,14 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
     float2* T2 = tw + L;               // kT2: [Q][P], T2[t * P + k1] = W_L^(t k1)
     float2* Y = T2 + (kT2 ? L : 0);    // [L][CWp] transpose buffer
     float2* acc = Y + L * CWp;  // kSenseReduce: [A_blk][groups][Lout] running sums
-    constexpr bool kPf = Prefetch<Op>::value;
-    static_assert(!kPf || (kHalfIn && Op::kFusedK && !StageRow<Op>::value), "prefetch: fused passes on padded inputs");
+    constexpr bool kPf = PF;
+    static_assert(!kPf || (Prefetch<Op>::value && (kHalfIn || kFullIn) && !StageRow<Op>::value && !Op::kLoadLFast),
+                  "prefetch: operators with fixed input positions and column-fast loads");
+    constexpr int kPfRows = kHalfIn ? L / 2 : L;
     float2* Ks = acc + (Op::kSenseReduce ? c.A_blk * op.ngroups() * c.Lout : 0);  // kFusedK: [max_kcols][L]
-    float2* Ss = Ks + (Op::kFusedK ? max_kcols<Op>() * L : 0);    // kSenseReduce: [W][Lout]
+    float2* Ss = Ks + (Op::kFusedK ? max_kcols<PF>() * L : 0);    // kSenseReduce: [W][Lout]
     float2* Rs = Ss + (Op::kSenseReduce ? c.W * c.Lout : 0);      // StageRow: [A_blk][L/2]
-    float2* Pf = Rs + (StageRow<Op>::value ? c.A_blk * (L / 2) : 0);  // kPf: [L/2][kCW] samples
+    float2* Pf = Rs + (StageRow<Op>::value ? c.A_blk * (L / 2) : 0);  // kPf: [kPfRows][kCW] samples
 
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
         tw[i] = c.tw[i];
@@ -240,35 +246,50 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
     const int out_shift = ((c.out_shift % L) + L) % L;
     __syncthreads();
 
-    int64_t ab, eb_begin, eb_end, eb_step = 1;
-    if (kPf) {
-        // one outer row (A == 1, A_blk == 1: checked by the launcher); blocks blockIdx.x, +gridDim.x, ...
+    // jobs (outer row block ab, inner column block eb) of this CTA: the first, then advance() to
+    // the next. A prefetching operator without a chunk loop has one outer row (A == 1, checked by
+    // the launcher) and strides over its column blocks; with a chunk loop it strides over rows and
+    // takes every block of a row.
+    const int64_t n_ab = (c.A + c.A_blk - 1) / c.A_blk;
+    int64_t ab = 0, eb = 0;
+    if constexpr (kPf && !Op::kChunkLoop) {
         ab = 0;
-        eb_begin = blockIdx.x;
-        eb_end = c.n_eb;
-        eb_step = gridDim.x;
-    } else if (Op::kChunkLoop) {
-        ab = blockIdx.x;
-        eb_begin = 0;
-        eb_end = c.n_eb;
+        eb = blockIdx.x;
+    } else if constexpr (Op::kChunkLoop) {
+        ab = blockIdx.x;  // kPf: rows blockIdx.x, +gridDim.x, ..., every block of a row here
+        eb = 0;
     } else {
         ab = blockIdx.x / c.n_eb;
-        eb_begin = blockIdx.x % c.n_eb;
-        eb_end = eb_begin + 1;
+        eb = blockIdx.x % c.n_eb;
     }
-    const int64_t a0 = ab * c.A_blk;
-    // kPf: the samples l < L/2 of block eb's kCW columns into Pf[l][col] (16-byte copies of two
-    // columns where both exist and are aligned, else one column at a time; missing columns are 0)
-    auto prefetch = [&](int64_t eb) {
+    bool have = (kPf && !Op::kChunkLoop) ? eb < c.n_eb : ab < n_ab;
+    auto advance = [&](int64_t& abj, int64_t& ebj) -> bool {
+        if constexpr (kPf && !Op::kChunkLoop) {
+            ebj += gridDim.x;
+            return ebj < c.n_eb;
+        } else if constexpr (Op::kChunkLoop) {
+            if (++ebj < c.n_eb) return true;
+            if (!kPf) return false;
+            ebj = 0;
+            abj += gridDim.x;
+            return abj < n_ab;
+        } else {
+            return false;
+        }
+    };
+    // kPf: the samples l < kPfRows of job (row a, block eb)'s kCW columns into Pf[l][col] (16-byte
+    // copies of two columns where both exist and are aligned, else one column at a time; missing
+    // columns are 0)
+    auto prefetch = [&](int64_t a, int64_t eb) {
         if constexpr (kPf) {
             const int64_t e0p = eb * c.E_blk;
             constexpr int PC = kCW / 2;
 #pragma unroll 1
-            for (int i = tid; i < (L / 2) * PC; i += blockDim.x) {
+            for (int i = tid; i < kPfRows * PC; i += blockDim.x) {
                 const int l = i / PC, pc = i - l * PC;
                 const int64_t e = e0p + 2 * pc;
                 float2* dst = Pf + l * kCW + 2 * pc;
-                const float2* src = op.src(l, e);
+                const float2* src = op.sample_ptr(a, l, e);
                 if (e + 1 < c.E && ((uintptr_t)src & 15) == 0) {
                     cp_async16(dst, src);
                 } else {
@@ -279,7 +300,7 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
             cp_async_commit();
         }
     };
-    if (kPf && eb_begin < eb_end) prefetch(eb_begin);
+    if (kPf && have) prefetch(ab * c.A_blk, eb);
     // column -> (row in the block, inner index); with one row per CTA (every large problem) the
     // runtime division by E_blk is skipped
     auto split_col = [&](int col, int& al, int& el) {
@@ -296,8 +317,16 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
         __syncthreads();
     }
 
-    for (int64_t eb = eb_begin; eb < eb_end; eb += eb_step) {
+    while (have) {
+        const int64_t a0 = ab * c.A_blk;
         const int64_t e0 = eb * c.E_blk;
+        int64_t ab_n = ab, eb_n = eb;
+        const bool next = advance(ab_n, eb_n);
+        if constexpr (kPf && !Op::kFusedK) {
+            // this job's samples (the only copies in flight)
+            cp_async_wait_all();
+            __syncthreads();
+        }
         // ---- stage the kernel columns / factor rows this chunk needs (asynchronous) -----------
         int64_t kc0 = 0;
         bool k_staged = false;
@@ -306,16 +335,16 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
             const int64_t elast = min(e0 + c.E_blk, c.E) - 1;
             kc0 = op.kcol(e0);
             nk = (int)(op.kcol(elast) - kc0 + 1);
-            k_staged = (c.A_blk == 1) && nk <= max_kcols<Op>();
+            k_staged = (c.A_blk == 1) && nk <= max_kcols<PF>();
             if (k_staged) {
                 for (int i = tid; i < nk * L; i += blockDim.x) cp_async8(Ks + i, op.kptr(kc0 + i / L) + (i % L));
                 cp_async_commit();
             }
-        }
-        if constexpr (kPf) {
-            // this block's samples (the group before the kernel columns just issued)
-            if (k_staged) cp_async_wait_group<1>(); else cp_async_wait_all();
-            __syncthreads();
+            if constexpr (kPf) {
+                // this job's samples: the group before the kernel columns just issued
+                if (k_staged) cp_async_wait_group<1>(); else cp_async_wait_all();
+                __syncthreads();
+            }
         }
         if constexpr (Op::kSenseReduce) {
             // one warp per column row: the row pointer once, then contiguous copies
@@ -389,6 +418,10 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 for (int j = 0; j < P; ++j)
                     v[j] = (j < P / 2 && colok) ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
                 halfzero = true;
+            } else if constexpr (kFullIn && kPf) {
+#pragma unroll
+                for (int j = 0; j < P; ++j) v[j] = Pf[(t + Q * j) * kCW + col];
+                halfzero = false;
             } else if constexpr (kFullIn) {
 #pragma unroll
                 for (int j = 0; j < P; ++j) v[j] = colok ? op.load(a, t + Q * j, e) : make_float2(0.f, 0.f);
@@ -427,8 +460,8 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
         }
         if (Op::kFusedK || Op::kSenseReduce) cp_async_wait_all();
         __syncthreads();
-        // every thread has read Pf: the next block's samples load while this one is transformed
-        if (kPf && eb + eb_step < eb_end) prefetch(eb + eb_step);
+        // every thread has read Pf: the next job's samples load while this one is transformed
+        if (kPf && next) prefetch(ab_n * c.A_blk, eb_n);
         // ---- step 2: thread (col, k1) runs the Q-point DFT ----------------------------------------
         const bool s2active = tid < P * kCW;
         int col2 = 0, k1 = 0;
@@ -591,17 +624,24 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
                 }
             }
         }
-        if (eb + eb_step < eb_end) __syncthreads();  // the next chunk rewrites Y (and the staged rows)
-    }
-    if constexpr (Op::kSenseReduce) {
-        __syncthreads();
-        const int ng = op.ngroups();
-        const int tot = c.A_blk * ng * c.Lout;
-        for (int idx = tid; idx < tot; idx += blockDim.x) {
-            const int o = idx % c.Lout, rest = idx / c.Lout, gg = rest % ng, al = rest / ng;
-            const int64_t a = a0 + al;
-            if (a < c.A) op.write_row(a, o, gg, acc[idx]);
+        if constexpr (Op::kSenseReduce) {
+            // the row block's last chunk: write its sums and clear them for the next row block
+            if (!next || ab_n != ab) {
+                __syncthreads();
+                const int ng = op.ngroups();
+                const int tot = c.A_blk * ng * c.Lout;
+                for (int idx = tid; idx < tot; idx += blockDim.x) {
+                    const int o = idx % c.Lout, rest = idx / c.Lout, gg = rest % ng, al = rest / ng;
+                    const int64_t a = a0 + al;
+                    if (a < c.A) op.write_row(a, o, gg, acc[idx]);
+                    acc[idx] = make_float2(0.f, 0.f);
+                }
+            }
         }
+        if (next) __syncthreads();  // the next job rewrites Y, the staged rows and the sums
+        ab = ab_n;
+        eb = eb_n;
+        have = next;
     }
 }
 
@@ -628,26 +668,27 @@ struct HalfIO<Op, std::void_t<decltype(Op::kHalfIO)>> {
     static constexpr int value = Op::kHalfIO;
 };
 
-template <int P, int Q, class Op, int HM>
+template <int P, int Q, class Op, int HM, bool PF>
 int launch_pass2_inst(const Op& op, const PassCfg& c, size_t smem, int64_t blocks, cudaStream_t s, const char* name) {
-    cudaError_t e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op, HM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = pass2_kernel<P, Q, Op, HM, PF>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // the staging passes want every CTA they can fit; plain passes keep the default L1 split
-    if (e == cudaSuccess && (Op::kFusedK || Op::kSenseReduce))
-        e = cudaFuncSetAttribute(pass2_kernel<P, Q, Op, HM>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess && (Op::kFusedK || Op::kSenseReduce || PF))
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) {
         set_error(std::string(name) + ": cudaFuncSetAttribute failed: " + cudaGetErrorString(e));
         return HB_ERR_CUDA;
     }
     int64_t grid = blocks;
-    if constexpr (Prefetch<Op>::value) {
-        // persistent CTAs: as many as are resident at once
+    if constexpr (PF) {
+        // persistent CTAs: as many as are resident at once (the shared bytes of a prefetching
+        // instance depend only on its template arguments)
         static int per_sm = 0, sms = 0;
         if (per_sm == 0) {
             int dev = 0, n = 0, m = 0;
             if (cudaGetDevice(&dev) != cudaSuccess ||
                 cudaDeviceGetAttribute(&m, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pass2_kernel<P, Q, Op, HM>, Q * kCW, smem) != cudaSuccess) {
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, Q * kCW, smem) != cudaSuccess) {
                 set_error(std::string(name) + ": occupancy query failed");
                 return HB_ERR_CUDA;
             }
@@ -657,7 +698,7 @@ int launch_pass2_inst(const Op& op, const PassCfg& c, size_t smem, int64_t block
         grid = std::min<int64_t>(blocks, (int64_t)per_sm * sms);
     }
     TimedSection ts(name, s);
-    pass2_kernel<P, Q, Op, HM><<<(unsigned)grid, Q * kCW, smem, s>>>(op, c);
+    kern<<<(unsigned)grid, Q * kCW, smem, s>>>(op, c);
     return check_launch(name);
 }
 
@@ -675,30 +716,33 @@ int launch_pass2_pq(const Op& op, PassCfg c, size_t extra_bytes, cudaStream_t s,
             return HB_ERR_INVALID_ARG;
         }
     }
+    // prefetching where the operator asks for it and a CTA holds one outer row of kCW-column blocks
+    // (or the whole row); the other shapes run the plain instance
+    constexpr bool kPfOp = Prefetch<Op>::value && HM != 0;
+    const bool pf = kPfOp && c.A_blk == 1 && (c.E_blk == kCW || c.n_eb == 1) && (Op::kChunkLoop || c.A == 1);
     size_t smem = (size_t)((Op::kFusedK || !Op::kLoadLFast ? 2 : 1) * L + L * (kCW + 1)) * sizeof(float2) + extra_bytes;
-    if (Op::kFusedK) smem += (size_t)max_kcols<Op>() * L * sizeof(float2);
-    if (Prefetch<Op>::value) smem += (size_t)(L / 2) * kCW * sizeof(float2);
+    if (Op::kFusedK) smem += (size_t)(pf ? max_kcols<true>() : max_kcols<false>()) * L * sizeof(float2);
+    if (pf) smem += (size_t)((HM & 1) ? L / 2 : L) * kCW * sizeof(float2);
     if (Op::kSenseReduce) smem += (size_t)c.W * c.Lout * sizeof(float2);
     if (StageRow<Op>::value) smem += (size_t)c.A_blk * (L / 2) * sizeof(float2);
     const int64_t n_ab = ceil_div(c.A, c.A_blk);
     const int64_t blocks = Op::kChunkLoop ? n_ab : n_ab * c.n_eb;
-    if (Prefetch<Op>::value && (c.A != 1 || c.A_blk != 1 || (c.E_blk != kCW && c.n_eb != 1))) {
-        set_error(std::string(name) + ": a prefetching pass takes one outer row of kCW-column blocks");
-        return HB_ERR_INVALID_ARG;
-    }
     if (blocks <= 0) return HB_OK;
     if (blocks > 0x7fffffffLL) {
         set_error(std::string(name) + ": grid too large");
         return HB_ERR_INVALID_ARG;
     }
     if constexpr (HM != 0) {
-        return launch_pass2_inst<P, Q, Op, HM>(op, c, smem, blocks, s, name);
+        if constexpr (kPfOp) {
+            if (pf) return launch_pass2_inst<P, Q, Op, HM, true>(op, c, smem, blocks, s, name);
+        }
+        return launch_pass2_inst<P, Q, Op, HM, false>(op, c, smem, blocks, s, name);
     } else {
         // no fixed shape: a side that spans all L positions unshifted gets compile-time positions
-        if (full_in && full_out) return launch_pass2_inst<P, Q, Op, 12>(op, c, smem, blocks, s, name);
-        if (full_in) return launch_pass2_inst<P, Q, Op, 4>(op, c, smem, blocks, s, name);
-        if (full_out) return launch_pass2_inst<P, Q, Op, 8>(op, c, smem, blocks, s, name);
-        return launch_pass2_inst<P, Q, Op, 0>(op, c, smem, blocks, s, name);
+        if (full_in && full_out) return launch_pass2_inst<P, Q, Op, 12, false>(op, c, smem, blocks, s, name);
+        if (full_in) return launch_pass2_inst<P, Q, Op, 4, false>(op, c, smem, blocks, s, name);
+        if (full_out) return launch_pass2_inst<P, Q, Op, 8, false>(op, c, smem, blocks, s, name);
+        return launch_pass2_inst<P, Q, Op, 0, false>(op, c, smem, blocks, s, name);
     }
 }
 
