@@ -4,15 +4,15 @@
 // 8 transforms, or one part of a dense tile's points. It copies the region the tile's footprints
 // can reach -- the tile plus W-1 cells above it along every axis, wrapped at the grid edge -- into
 // shared memory (cp.async, 16-byte pieces of 2 transforms), stages its points' tap weights, and
-// then every lane group of 8 lanes (one point, 8 transforms) gathers the point's W^3 cells from
-// shared memory at compile-time offsets: no wrap or bounds logic in the gather.
+// then every group of 4 lanes (one point, 2 transforms per lane) gathers the point's W^3 cells
+// from shared memory at compile-time offsets: no wrap or bounds logic in the gather.
 //
 // Bank layout: a cell is 8 transforms x 8 B = 64 B, half of the 128-byte bank window, and the
 // region's row pitches are odd, so a cell's half of the banks is the parity of z + y + x. Every tap
-// of a point keeps the parity of its first cell. An 8-byte load is served per half-warp (two lane
-// groups), so a half-warp whose two groups hold points of opposite parity reads its two cells in
-// one wavefront: the minimum two per warp load. The CTA orders its points into such quadruples
-// (even, odd, even, odd) and runs the unmatched rest after them.
+// of a point keeps the parity of its first cell. A 16-byte load is served per quarter-warp (two lane
+// groups), so a quarter-warp whose two groups hold points of opposite parity reads its two cells
+// in one wavefront: the minimum four per warp load. The CTA orders its points into such pairs
+// (even, odd) and runs the unmatched rest after them.
 //
 // The sums run in the order of the gathering kernel (per row the x taps, then the row weight
 // w_z w_y), with the same tap weights, so both kernels give bit-identical samples.
@@ -26,7 +26,7 @@
 namespace hb {
 
 constexpr int kStCoils = 8;      // transforms per CTA
-constexpr int kStThreads = 512;  // 16 warps x 4 lane groups
+constexpr int kStThreads = 512;  // 16 warps x 8 lane groups
 
 template <int W>
 struct StShape {
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
     float* rec = coef + kCoefFloats;
     int* rel = reinterpret_cast<int*>(rec + S::kMaxPts * S::kRecF);  // packed region-relative first cells
     int* pidx = rel + S::kMaxPts;                                    // caller's index of the point
-    int* order = pidx + S::kMaxPts;                                  // visit order (parity quadruples)
+    int* order = pidx + S::kMaxPts;                                  // visit order (parity pairs)
     __shared__ int s_cnt[2];
     const GridGeom& g = a.g;
     const int tid = threadIdx.x;
@@ -69,23 +69,35 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
 
     if (tid < 2) s_cnt[tid] = 0;
     for (int i = tid; i < kCoefFloats; i += kStThreads) coef[i] = (&a.kb.coef[0][0])[i];
-    // the region: R^3 cells x 4 pieces of 2 transforms
+    // the region: one warp per (z, y) row of R cells x 4 pieces of 2 transforms; every wrapped
+    // coordinate needs at most two subtractions (org + r < 8 nb + 15 <= 3 nf)
     const bool vec = (g.C % 2) == 0;
-    for (int i = tid; i < R * R * R * 4; i += kStThreads) {
-        const int pc = i & 3, cell = i >> 2;
-        const int x = cell % R, y = (cell / R) % R, z = cell / (R * R);
-        int gz = org0 + z, gy = org1 + y, gx = org2 + x;
-        while (gz >= nf0) gz -= nf0;
-        while (gy >= nf1) gy -= nf1;
-        while (gx >= nf2) gx -= nf2;
-        const int c = cc0 + 2 * pc;
-        const float2* src = a.grid + (((int64_t)gz * nf1 + gy) * nf2 + gx) * g.C + c;
-        float2* dst = region + ((z * RP + y) * RP + x) * kStCoils + 2 * pc;
-        if (vec && c < g.C) {
-            cp_async16(dst, src);
-        } else {
-            if (c < g.C) cp_async8(dst, src); else dst[0] = make_float2(0.f, 0.f);
-            if (c + 1 < g.C) cp_async8(dst + 1, src + 1); else dst[1] = make_float2(0.f, 0.f);
+    {
+        const int warp = tid >> 5, lane = tid & 31;
+        for (int row = warp; row < R * R; row += kStThreads / 32) {
+            const int z = row / R, y = row - z * R;
+            int gz = org0 + z, gy = org1 + y;
+            if (gz >= nf0) gz -= nf0;
+            if (gz >= nf0) gz -= nf0;
+            if (gy >= nf1) gy -= nf1;
+            if (gy >= nf1) gy -= nf1;
+            const float2* srow = a.grid + ((int64_t)gz * nf1 + gy) * nf2 * g.C + cc0;
+            float2* drow = region + (z * RP + y) * RP * kStCoils;
+            for (int i = lane; i < R * 4; i += 32) {
+                const int x = i >> 2, pc = i & 3;
+                int gx = org2 + x;
+                if (gx >= nf2) gx -= nf2;
+                if (gx >= nf2) gx -= nf2;
+                const int c = cc0 + 2 * pc;
+                const float2* src = srow + (int64_t)gx * g.C + 2 * pc;
+                float2* dst = drow + x * kStCoils + 2 * pc;
+                if (vec && c < g.C) {
+                    cp_async16(dst, src);
+                } else {
+                    if (c < g.C) cp_async8(dst, src); else dst[0] = make_float2(0.f, 0.f);
+                    if (c + 1 < g.C) cp_async8(dst + 1, src + 1); else dst[1] = make_float2(0.f, 0.f);
+                }
+            }
         }
     }
     cp_async_commit();
@@ -112,7 +124,7 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
         if (ax == 0) pidx[q] = a.perm[sidx];
     }
     __syncthreads();
-    // parity classes, then the visit order: quadruples (even, odd, even, odd), then the rest
+    // parity classes, then the visit order: pairs (even, odd), then the rest
     for (int q = tid; q < n; q += kStThreads) {
         const int pk = rel[q];
         const int par = ((pk & 0xff) + ((pk >> 8) & 0xff) + ((pk >> 16) & 0xff)) & 1;
@@ -122,58 +134,61 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
     __syncthreads();
     {
         const int ne = s_cnt[0], no = s_cnt[1];
-        const int m2 = min(ne, no) >> 1;  // matched quadruples
+        const int m = min(ne, no);  // matched pairs
         const int o = tid < n ? order[tid] : 0;
         __syncthreads();
         if (tid < n) {
             const int par = o >> 30, i = o & 0x3fffffff;
-            const int slot = i < 2 * m2 ? 4 * (i >> 1) + 2 * (i & 1) + par
-                                        : 4 * m2 + (par ? ne - 2 * m2 : 0) + (i - 2 * m2);
+            const int slot = i < m ? 2 * i + par : 2 * m + (par ? ne - m : 0) + (i - m);
             order[slot] = tid;
         }
     }
     cp_async_wait_all();
     __syncthreads();
 
-    // gathers: lane group = one point, lane = one transform
-    const int warp = tid >> 5, lane = tid & 31, grp = lane >> 3, c = lane & 7;
-    const bool cok = cc0 + c < g.C;
-    float2* outc = a.out + (int64_t)(cc0 + c) * g.M;
-    for (int base = 0; base < n; base += 64) {
-        const int o = base + warp * 4 + grp;
+    // gathers: a group of 4 lanes = one point, each lane 2 transforms (16-byte loads, served per
+    // quarter-warp: two points of opposite parity per quarter-warp, one wavefront)
+    const int warp = tid >> 5, lane = tid & 31, grp = lane >> 2, c2 = lane & 3;
+    const int cA = cc0 + 2 * c2;
+    float2* outA = a.out + (int64_t)cA * g.M;
+    float2* outB = outA + g.M;
+    for (int base = 0; base < n; base += kStThreads / 4) {
+        const int o = base + warp * 8 + grp;
         if (o >= n) continue;
         const int q = order[o];
         const int pk = rel[q];
         const int rz = pk & 0xff, ry = (pk >> 8) & 0xff, rx = (pk >> 16) & 0xff;
         const float* rq = rec + q * S::kRecF;
-        float wy[W], wx[W];
+        float wx[W];
 #pragma unroll
-        for (int d = 0; d < W; ++d) {
-            wy[d] = rq[8 + d];
-            wx[d] = rq[16 + d];
-        }
-        const float2* p0 = region + ((rz * RP + ry) * RP + rx) * kStCoils + c;
-        float ar = 0.f, ai = 0.f;
-        // one W x W slab of gathers in flight per step (all W^3 at once would spill)
+        for (int d = 0; d < W; ++d) wx[d] = rq[16 + d];
+        const float4* p0 = reinterpret_cast<const float4*>(region + ((rz * RP + ry) * RP + rx) * kStCoils) + c2;
+        float ar0 = 0.f, ai0 = 0.f, ar1 = 0.f, ai1 = 0.f;
 #pragma unroll 1
         for (int dz = 0; dz < W; ++dz) {
             const float wzd = rq[dz];
-#pragma unroll
+#pragma unroll 2
             for (int dy = 0; dy < W; ++dy) {
-                const float2* pr = p0 + (dz * RP + dy) * RP * kStCoils;
-                float rr = 0.f, ri = 0.f;
+                const float4* pr = p0 + (dz * RP + dy) * RP * (kStCoils / 2);
+                float rr0 = 0.f, ri0 = 0.f, rr1 = 0.f, ri1 = 0.f;
 #pragma unroll
                 for (int dx = 0; dx < W; ++dx) {
-                    const float2 v = pr[dx * kStCoils];
-                    rr = fmaf(wx[dx], v.x, rr);
-                    ri = fmaf(wx[dx], v.y, ri);
+                    const float4 v = pr[dx * (kStCoils / 2)];
+                    rr0 = fmaf(wx[dx], v.x, rr0);
+                    ri0 = fmaf(wx[dx], v.y, ri0);
+                    rr1 = fmaf(wx[dx], v.z, rr1);
+                    ri1 = fmaf(wx[dx], v.w, ri1);
                 }
-                const float wzy = wzd * wy[dy];
-                ar = fmaf(wzy, rr, ar);
-                ai = fmaf(wzy, ri, ai);
+                const float wzy = wzd * rq[8 + dy];
+                ar0 = fmaf(wzy, rr0, ar0);
+                ai0 = fmaf(wzy, ri0, ai0);
+                ar1 = fmaf(wzy, rr1, ar1);
+                ai1 = fmaf(wzy, ri1, ai1);
             }
         }
-        if (cok) outc[pidx[q]] = make_float2(ar, ai);
+        const int pj = pidx[q];
+        if (cA < g.C) outA[pj] = make_float2(ar0, ai0);
+        if (cA + 1 < g.C) outB[pj] = make_float2(ar1, ai1);
     }
 }
 
