@@ -487,7 +487,10 @@ def bench_frames(args, hb, dev, stream, world=1, rank=0, nframes=24, shape=(128,
     - batched: one graph-captured CG over all frames (all frames and coils in one launch per pass);
     - Toeplitz loop: a graph-captured CG on the single-frame fused operator, frame after frame;
     - plain loop: CG on the plain NUFFT SENSE operator (type 2 then type 1 per apply), frame after
-      frame, with the adjoint's spreading autotuned for the problem.
+      frame, with the adjoint's spreading autotuned for the problem;
+    - plain batched: the same plain operator over groups of frames, each group one frame-batched
+      NUFFT plan pair (one launch per pass over all its frames' points) and one batched CG.
+    The per-frame Toeplitz kernels are built frame-batched (build_toeplitz_kernels).
     With several ranks every rank reconstructs its share of the frames (split by sample count) and
     the times are the slowest rank's."""
     import torch
@@ -577,6 +580,26 @@ def bench_frames(args, hb, dev, stream, world=1, rank=0, nframes=24, shape=(128,
             xl[i] = sv.solve(x0[i], b[i])
 
     t_loop = timed_region(plain_loop)
+    del sv
+    # frame-batched plain operator: groups of frames share one NUFFT plan pair (every pass of a
+    # type 2 / type 1 covers the group's points in one launch) and one CG over the group's frames;
+    # the group is bounded by the plans' grids (about 3.2 GB per frame and plan at 128^3 x 16 coils)
+    G = max(g for g in range(1, min(F, 6) + 1) if F % g == 0)
+    bso = hb.BatchedSenseOp([dcoords[i] for i in range(G)], S, kernel_width=w, scale=1.0 / math.sqrt(n),
+                            spread_tuning=tune)
+    bsv = hb.BatchedCGSolver(lambda v, o: o.copy_(bso.normal(v)), G, shape, dev, max_iter=iters, tol=0.0)
+    bsv.solve(x0[:G], b[:G])  # warm-up
+    xpb = torch.empty_like(xb)
+
+    def plain_batched():
+        for g0 in range(0, F, G):
+            bso.setpts([dcoords[i] for i in range(g0, g0 + G)])
+            xpb[g0: g0 + G] = bsv.solve(x0[g0: g0 + G], b[g0: g0 + G])
+
+    t_pb = timed_region(plain_batched)
+    pdiff = float(torch.linalg.vector_norm(xpb - xl) / torch.linalg.vector_norm(xl))
+    del bsv, bso
+    torch.cuda.empty_cache()
     diff = float(torch.linalg.vector_norm(xb - xl) / torch.linalg.vector_norm(xl))
     tdiff = float(torch.linalg.vector_norm(xb - xt) / torch.linalg.vector_norm(xt))
     return {"workload": f"{nframes} frames x {shape[0]}^3, {C} coils, golden-means radial 300-700 spokes x 128, "
@@ -585,6 +608,9 @@ def bench_frames(args, hb, dev, stream, world=1, rank=0, nframes=24, shape=(128,
             "batched_recons_per_s": round(nframes / t_batched, 3), "batched_s": round(t_batched, 3),
             "toeplitz_looped_recons_per_s": round(nframes / t_tloop, 3), "toeplitz_looped_s": round(t_tloop, 3),
             "plain_looped_recons_per_s": round(nframes / t_loop, 3), "plain_looped_s": round(t_loop, 3),
+            "plain_batched_recons_per_s": round(nframes / t_pb, 3), "plain_batched_s": round(t_pb, 3),
+            "plain_batched_frames_per_plan": G, "plain_batching_gain": round(t_loop / t_pb, 3),
+            "plain_batched_vs_plain_looped_rel_diff": pdiff,
             "batching_gain": round(t_tloop / t_batched, 3), "toeplitz_gain": round(t_loop / t_tloop, 3),
             "speedup_vs_plain_loop": round(t_loop / t_batched, 2),
             "batched_vs_toeplitz_looped_rel_diff": tdiff, "batched_vs_plain_looped_rel_diff": diff,

@@ -21,12 +21,14 @@ from .toeplitz import (  # noqa: F401
     sense_normal,
     sense_normal_ex,
     toeplitz_kernel,
+    toeplitz_kernels_frames,
     toeplitz_multiplication,
     toeplitz_multiply,
     transform_toeplitz_kernel,
 )
 from .normal import (  # noqa: F401
     BatchedNormalOp,
+    BatchedSenseOp,
     NormalIDTT1Op,
     NormalIDTT2Op,
     NormalIDTWT1Op,

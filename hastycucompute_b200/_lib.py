@@ -32,6 +32,7 @@ SIGNATURES = {
     "hb_version": (_i, []),
     "hb_nufft_makeplan": (_i, [_i, _i, _pi64, _i, _i, _f, _i, _d, _i, C.POINTER(_vp)]),
     "hb_nufft_setpts": (_i, [_vp, _i64, _vp, _vp, _vp, _vp]),
+    "hb_nufft_setpts_frames": (_i, [_vp, _i, _pi64, _vp, _vp, _vp, _vp]),
     "hb_nufft_execute": (_i, [_vp, _vp, _vp, _vp]),
     "hb_nufft_destroy": (_i, [_vp]),
     "hb_nufft_coord_grad": (_i, [_vp, _vp, _vp, _vp, _vp]),
@@ -41,6 +42,7 @@ SIGNATURES = {
     "hb_nufft_set_interp_kernel": (_i, [_vp, _i]),
     "hb_nufft_get_info": (_i, [_vp, _pi64, C.POINTER(_i), C.POINTER(_d), C.POINTER(_sz)]),
     "hb_toeplitz_kernel": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
+    "hb_toeplitz_kernels_frames": (_i, [_i, _pi64, _i, _pi64, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "hb_transform_toeplitz_kernel": (_i, [_i, _pi64, _vp, _vp, _vp]),
     "hb_toeplitz_workspace_size": (_i, [_i, _pi64, _i64, C.POINTER(_sz)]),
     "hb_toeplitz_multiplication": (_i, [_i, _pi64, _i64, _vp, _vp, _vp, _vp, _sz, _vp, _vp,

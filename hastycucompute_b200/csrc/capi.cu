@@ -15,6 +15,8 @@ const char* get_error() { return g_last_error.c_str(); }
 // implemented in toeplitz.cu / cg.cu
 int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, const float* c1, const float* c2,
                     const void* nudata, void* kout, int width, cudaStream_t s);
+int toeplitz_kernel_frames(int dim, const int64_t* kshape, int nframes, const int64_t* npts, const float* c0,
+                           const float* c1, const float* c2, const void* nudata, void* kout, int width, cudaStream_t s);
 int transform_toeplitz_kernel(int dim, const int64_t* kshape, const void* kin, void* kout, cudaStream_t s);
 int toeplitz_workspace_size(int dim, const int64_t* shape, int64_t nbatch, size_t* bytes);
 int toeplitz_multiplication(int dim, const int64_t* shape, int64_t nbatch, const void* input, void* output,
@@ -103,6 +105,17 @@ int hb_nufft_setpts(hb_nufft_plan plan, int64_t M, const float* coord0, const fl
             return HB_ERR_INVALID_ARG;
         }
         return hb::plan_setpts(&plan->p, M, coord0, coord1, coord2, as_stream(stream));
+    })
+}
+
+int hb_nufft_setpts_frames(hb_nufft_plan plan, int nframes, const int64_t* npts, const float* coord0,
+                           const float* coord1, const float* coord2, void* stream) {
+    HB_GUARD({
+        if (!plan) {
+            hb::set_error("plan is null");
+            return HB_ERR_INVALID_ARG;
+        }
+        return hb::plan_setpts_frames(&plan->p, nframes, npts, coord0, coord1, coord2, as_stream(stream));
     })
 }
 
@@ -199,6 +212,15 @@ int hb_toeplitz_kernel(int dim, const int64_t* kernel_shape, int64_t M, const fl
     HB_GUARD({
         return hb::toeplitz_kernel(dim, kernel_shape, M, coord0, coord1, coord2, nudata, kernel_out, kernel_width,
                                    as_stream(stream));
+    })
+}
+
+int hb_toeplitz_kernels_frames(int dim, const int64_t* kernel_shape, int nframes, const int64_t* npts,
+                               const float* coord0, const float* coord1, const float* coord2, const void* nudata,
+                               void* kernel_out, int kernel_width, void* stream) {
+    HB_GUARD({
+        return hb::toeplitz_kernel_frames(dim, kernel_shape, nframes, npts, coord0, coord1, coord2, nudata, kernel_out,
+                                          kernel_width, as_stream(stream));
     })
 }
 

@@ -61,8 +61,11 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
     const GridGeom& g = a.g;
     const int tid = threadIdx.x;
     const int4 job = jobs[blockIdx.x];
-    const int tile = job.x, k0 = job.y, n = job.z - job.y;
+    int tile = job.x;
+    const int k0 = job.y, n = job.z - job.y;
     const int cc0 = (int)blockIdx.y * kStCoils;
+    const int fr = split_frame_tile(g, tile);
+    const float2* const gridf = a.grid + fr * g.fgrid;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int org0 = tz * 8, org1 = ty * 8, org2 = tx * 8;
     const int nf0 = g.nf[0], nf1 = g.nf[1], nf2 = g.nf[2];
@@ -81,7 +84,7 @@ __global__ void __launch_bounds__(kStThreads, 1) k_interp_st(const GridArgs a, c
             if (gz >= nf0) gz -= nf0;
             if (gy >= nf1) gy -= nf1;
             if (gy >= nf1) gy -= nf1;
-            const float2* srow = a.grid + ((int64_t)gz * nf1 + gy) * nf2 * g.C + cc0;
+            const float2* srow = gridf + ((int64_t)gz * nf1 + gy) * nf2 * g.C + cc0;
             float2* drow = region + (z * RP + y) * RP * kStCoils;
             for (int i = lane; i < R * 4; i += 32) {
                 const int x = i >> 2, pc = i & 3;

@@ -60,6 +60,9 @@ struct FoldArgs {
     float scale[3];
     float hw;
     int64_t M;
+    const int* foff;  // frame point offsets (nullptr: one frame)
+    int nfr;
+    int ntf;          // bins per frame
 };
 
 __device__ __forceinline__ float fold_fine(float x, float scale, int nf) {
@@ -98,7 +101,7 @@ __global__ void k_fold_bin(const FoldArgs a) {
         a.u[ax][j] = u;
         b[ax] = first_cell(u, a.hw, a.nf[ax]) / a.T[ax];
     }
-    const int bin = (b[0] * a.nb[1] + b[1]) * a.nb[2] + b[2];
+    const int bin = (b[0] * a.nb[1] + b[1]) * a.nb[2] + b[2] + frame_of_point(a.foff, a.nfr, j) * a.ntf;
     a.binid[j] = bin;
     a.rank[j] = atomicAdd(&a.count[bin], 1);
 }
@@ -192,6 +195,8 @@ int exclusive_scan_int(const int* in, int* out, int64_t n, cudaStream_t s, int* 
 // ---- spread work list --------------------------------------------------------------------------
 struct TileNbr {
     int nb[3];
+    int nfr;  // frames
+    int ntf;  // tiles per frame
 };
 
 // Visits the (up to 8) bins whose points can reach tile (tz, ty, tx): along each axis with more
@@ -214,9 +219,10 @@ __device__ __forceinline__ void for_each_nbr_bin(const int* nb, int tz, int ty, 
 __global__ void k_tile_extra_count(const int* bin_start, TileNbr t, int64_t ntiles, int maxp, int* extra_cnt) {
     const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tile >= ntiles) return;
-    const int tx = (int)(tile % t.nb[2]), ty = (int)((tile / t.nb[2]) % t.nb[1]), tz = (int)(tile / ((int64_t)t.nb[2] * t.nb[1]));
+    const int64_t fr = t.nfr > 1 ? tile / t.ntf : 0, lt = tile - fr * t.ntf, fb = fr * t.ntf;
+    const int tx = (int)(lt % t.nb[2]), ty = (int)((lt / t.nb[2]) % t.nb[1]), tz = (int)(lt / ((int64_t)t.nb[2] * t.nb[1]));
     int64_t total = 0;
-    for_each_nbr_bin(t.nb, tz, ty, tx, [&](int bin) { total += bin_start[bin + 1] - bin_start[bin]; });
+    for_each_nbr_bin(t.nb, tz, ty, tx, [&](int bin) { total += bin_start[fb + bin + 1] - bin_start[fb + bin]; });
     const int64_t nsub = total > 0 ? (total + maxp - 1) / maxp : 1;
     extra_cnt[tile] = (int)(nsub - 1);
 }
@@ -235,9 +241,10 @@ __global__ void k_tile_extra_fill(const int* extra_cnt, const int* extra_off, in
 __global__ void k_tile_parts_count(const int* bin_start, TileNbr t, int64_t ntiles, int maxp, int* cnt) {
     const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tile >= ntiles) return;
-    const int tx = (int)(tile % t.nb[2]), ty = (int)((tile / t.nb[2]) % t.nb[1]), tz = (int)(tile / ((int64_t)t.nb[2] * t.nb[1]));
+    const int64_t fr = t.nfr > 1 ? tile / t.ntf : 0, lt = tile - fr * t.ntf, fb = fr * t.ntf;
+    const int tx = (int)(lt % t.nb[2]), ty = (int)((lt / t.nb[2]) % t.nb[1]), tz = (int)(lt / ((int64_t)t.nb[2] * t.nb[1]));
     int64_t total = 0;
-    for_each_nbr_bin(t.nb, tz, ty, tx, [&](int bin) { total += bin_start[bin + 1] - bin_start[bin]; });
+    for_each_nbr_bin(t.nb, tz, ty, tx, [&](int bin) { total += bin_start[fb + bin + 1] - bin_start[fb + bin]; });
     cnt[tile] = total > maxp ? (int)((total + maxp - 1) / maxp) : 0;
 }
 
@@ -330,6 +337,9 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
         tile = blockIdx.x;
         chunk = 0;
     }
+    const int fr = split_frame_tile(g, tile);
+    const int fbin = fr * (int)g.ntf;
+    float2* const gridf = a.grid + fr * g.fgrid;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int o0 = tz * T0, o1 = ty * T1, o2 = tx * T2;
 
@@ -337,10 +347,10 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
     if (threadIdx.x == 0) {
         int n = 0, acc = 0;
         for_each_nbr_bin(g.nb, tz, ty, tx, [&](int bin) {
-            const int st = a.bin_start[bin];
+            const int st = a.bin_start[fbin + bin];
             s_start[n] = st;
             s_pref[n] = acc;
-            acc += a.bin_start[bin + 1] - st;
+            acc += a.bin_start[fbin + bin + 1] - st;
             ++n;
         });
         s_pref[n] = acc;
@@ -411,7 +421,7 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
             if (cc0 + c >= g.C) continue;
             const int cx = cell % T2, cy = (cell / T2) % T1, cz = cell / (T1 * T2);
             const int64_t gi = ((int64_t)(o0 + cz) * g.nf[1] + (o1 + cy)) * g.nf[2] + (o2 + cx);
-            float2* dst = a.grid + gi * g.C + cc0 + c;
+            float2* dst = gridf + gi * g.C + cc0 + c;
             if (extra_mode) {
                 atomicAdd(&dst->x, acc_re[i]);
                 atomicAdd(&dst->y, acc_im[i]);
@@ -479,6 +489,9 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
         tile = blockIdx.x;
         chunk = 0;
     }
+    const int fr = split_frame_tile(g, tile);
+    const int fbin = fr * (int)g.ntf;
+    float2* const gridf = a.grid + fr * g.fgrid;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int org0 = tz * T0, org1 = ty * T1, org2 = tx * T2;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -507,8 +520,8 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
             const int bz = (tz - dz + g.nb[0]) % g.nb[0], by = (ty - dy + g.nb[1]) % g.nb[1];
             const int bx = (tx - dx + g.nb[2]) % g.nb[2];
             const int bin = (bz * g.nb[1] + by) * g.nb[2] + bx;
-            st = a.bin_start[bin];
-            cnt = a.bin_start[bin + 1] - st;
+            st = a.bin_start[fbin + bin];
+            cnt = a.bin_start[fbin + bin + 1] - st;
         }
         int incl = cnt;
 #pragma unroll
@@ -538,7 +551,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                 const int r = i / rowf4, c4 = i - r * rowf4;
                 const int zz = r / T1, yy = r - zz * T1;
                 float4* dst = reinterpret_cast<float4*>(
-                    a.grid + (((int64_t)(org0 + zz) * nf1 + (org1 + yy)) * nf2 + org2) * g.C);
+                    gridf + (((int64_t)(org0 + zz) * nf1 + (org1 + yy)) * nf2 + org2) * g.C);
                 dst[c4] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
         }
@@ -712,7 +725,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                     if (cg < g.C) {
                         const int64_t gi = ((int64_t)(org0 + jz) * nf1 + (org1 + jy)) * nf2 + (org2 + jx);
                         const float2 v = ow[j * (H + 1) + c];
-                        float2* dst = a.grid + gi * g.C + cg;
+                        float2* dst = gridf + gi * g.C + cg;
                         if (extra_mode)
                             atomicAdd(dst, v);
                         else
@@ -765,6 +778,7 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
                 wx[d] = wts[2 * kMaxWidth + d];
             }
             const int pj = a.perm[s];
+            const float2* const gridf = a.grid + frame_of_point(a.foff, g.nfr, s) * g.fgrid;
             const unsigned rowstride = (unsigned)nf2 * (unsigned)g.C;
             // Common case: the footprint wraps neither along axis 2 nor axis 1 and the lanes hold
             // all C transforms, so a tap's column stride is the compile-time CC: one row pointer,
@@ -773,7 +787,7 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
             const unsigned cs = (unsigned)g.C;  // column stride of a tap along axis 2
             for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
                 if (cc0 + coil >= g.C) break;
-                const float2* gridc = a.grid + cc0 + coil;
+                const float2* gridc = gridf + cc0 + coil;
                 float ar = 0.f, ai = 0.f;
                 for (int dz = 0; dz < wz; ++dz) {
                     int gz = i0[0] + dz;
@@ -923,10 +937,11 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_grad(const GridArgs a, 
                 dx_[d] = dwt[2 * kMaxWidth + d];
             }
             pj = a.perm[s];
+            const float2* const gridf = a.grid + frame_of_point(a.foff, g.nfr, s) * g.fgrid;
             const unsigned rowstride = (unsigned)nf2 * (unsigned)g.C;
             for (int cc0 = 0; cc0 < g.C; cc0 += CC) {
                 if (cc0 + coil >= g.C) break;
-                const float2* gridc = a.grid + cc0 + coil;
+                const float2* gridc = gridf + cc0 + coil;
                 float2 az = make_float2(0.f, 0.f), ay = az, axx = az;
                 for (int dz = 0; dz < wz; ++dz) {
                     int gz = i0[0] + dz;
@@ -993,9 +1008,11 @@ struct OpModesIn {
     const float* d2;
     int64_t N1, N2, nm;  // modes of axis 1, 2; modes per transform
     int64_t d_a, d_l;
+    int64_t rows_f, fstride;  // rows (N0 N1) and mode values (C nm) per frame
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
-        const float sc = d0[a / N1] * d1[a % N1] * d2[l];
-        return cscale(f[e * nm + a * N2 + l], sc);
+        const int64_t fr = a / rows_f, al = a - fr * rows_f;
+        const float sc = d0[al / N1] * d1[al % N1] * d2[l];
+        return cscale(f[fr * fstride + e * nm + al * N2 + l], sc);
     }
     __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
@@ -1030,6 +1047,7 @@ struct OpModesOut {
     const float* d2;
     int64_t N1, N2, nm;
     int64_t s_a, s_l;
+    int64_t rows_f, fstride;  // rows (N0 N1) and mode values (C nm) per frame
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
     __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
@@ -1039,8 +1057,9 @@ struct OpModesOut {
     __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
-        const float sc = d0[a / N1] * d1[a % N1] * d2[o];
-        f[e * nm + a * N2 + o] = cscale(v, sc);
+        const int64_t fr = a / rows_f, al = a - fr * rows_f;
+        const float sc = d0[al / N1] * d1[al % N1] * d2[o];
+        f[fr * fstride + e * nm + al * N2 + o] = cscale(v, sc);
     }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
     __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
@@ -1143,6 +1162,8 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
         return HB_ERR_INVALID_ARG;
     }
     p->nbins = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
+    g.nfr = 1;
+    g.ntf = p->nbins;
 
     // FFT plans and deapodisation factors per axis
     for (int ax = 0; ax < 3; ++ax) {
@@ -1162,9 +1183,12 @@ int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, 
     HB_REQUIRE(p->X_elems < ((size_t)1 << 32), HB_ERR_INVALID_ARG,
                "fine grid x ntransf must hold fewer than 2^32 values; split the transforms");
     p->Y_elems = (size_t)g.Nm[0] * g.nf[1] * g.nf[2] * g.C;
+    g.fgrid = (int64_t)p->X_elems;
+    p->frames_cap = 1;
     HB_TRY(dev_alloc(p, (void**)&p->X, sizeof(float2) * p->X_elems, "fine grid"));
     HB_TRY(dev_alloc(p, (void**)&p->Y, sizeof(float2) * p->Y_elems, "pass buffer"));
     HB_TRY(dev_alloc(p, (void**)&p->bin_start, sizeof(int) * (p->nbins + 1), "bins"));
+    p->nbins_cap = p->nbins;
     HB_TRY(dev_alloc(p, (void**)&p->d_err, sizeof(int), "error flag"));
     return HB_OK;
 }
@@ -1202,8 +1226,55 @@ static int st_build_jobs(NufftPlan* p, cudaStream_t s) {
 }
 
 int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const float* c2, cudaStream_t s) {
+    return plan_setpts_frames(p, 1, &M, c0, c1, c2, s);
+}
+
+int plan_setpts_frames(NufftPlan* p, int nframes, const int64_t* npts, const float* c0, const float* c1,
+                       const float* c2, cudaStream_t s) {
     GridGeom& g = p->g;
-    HB_REQUIRE(M >= 0 && M < (int64_t)0x7fffffff, HB_ERR_INVALID_ARG, "M must be in [0, 2^31)");
+    HB_REQUIRE(nframes >= 1 && nframes <= (1 << 16), HB_ERR_INVALID_ARG, "nframes must be in [1, 65536]");
+    HB_REQUIRE(npts != nullptr, HB_ERR_INVALID_ARG, "npts is null");
+    int64_t M = 0;
+    std::vector<int> hoff((size_t)nframes + 1, 0);
+    for (int f = 0; f < nframes; ++f) {
+        HB_REQUIRE(npts[f] >= 0, HB_ERR_INVALID_ARG, "a frame's point count is negative");
+        M += npts[f];
+        HB_REQUIRE(M < (int64_t)0x7fffffff, HB_ERR_INVALID_ARG, "M must be in [0, 2^31)");
+        hoff[(size_t)f + 1] = (int)M;
+    }
+    HB_REQUIRE((int64_t)p->g.ntf * nframes < (int64_t)0x7fffffff, HB_ERR_INVALID_ARG, "too many frames for the grid");
+    // grids and per-bin scratch for nframes frames (grown, never shrunk)
+    if (nframes > p->frames_cap) {
+        if (p->X) cudaFree(p->X);
+        if (p->Y) cudaFree(p->Y);
+        p->X = p->Y = nullptr;
+        p->frames_cap = 0;
+        p->pts_set = false;
+        HB_TRY(dev_alloc(p, (void**)&p->X, sizeof(float2) * p->X_elems * nframes, "fine grid (frames)"));
+        HB_TRY(dev_alloc(p, (void**)&p->Y, sizeof(float2) * p->Y_elems * nframes, "pass buffer (frames)"));
+        p->frames_cap = nframes;
+    }
+    const int64_t nbins_all = p->g.ntf * nframes;
+    if (nbins_all > p->nbins_cap) {
+        for (int** q : {&p->bin_start, &p->tmp_count, &p->tmp_ecnt, &p->tmp_eoff, &p->tmp_sums}) {
+            if (*q) cudaFree(*q);
+            *q = nullptr;
+        }
+        p->nbins_cap = 0;
+        p->pts_set = false;
+        HB_TRY(dev_alloc(p, (void**)&p->bin_start, sizeof(int) * (nbins_all + 1), "bins (frames)"));
+        p->nbins_cap = nbins_all;
+    }
+    if (nframes > 1 && nframes + 1 > p->foff_cap) {
+        if (p->foff) cudaFree(p->foff);
+        p->foff = nullptr;
+        p->foff_cap = 0;
+        HB_TRY(dev_alloc(p, (void**)&p->foff, sizeof(int) * (nframes + 1), "frame offsets"));
+        p->foff_cap = nframes + 1;
+    }
+    if (nframes > 1) HB_CUDA(cudaMemcpyAsync(p->foff, hoff.data(), sizeof(int) * (nframes + 1), cudaMemcpyHostToDevice, s));
+    g.nfr = nframes;
+    p->nbins = nbins_all;
     const float* cu[3] = {c0, c1, c2};
     const float* ca[3] = {nullptr, nullptr, nullptr};
     for (int i = 0; i < g.dim; ++i) {
@@ -1231,10 +1302,10 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
     // scratch held by the plan (allocated on the first setpts, per-point arrays grown with M)
     int st = HB_OK;
     if (p->tmp_count == nullptr) {
-        const int64_t nb = ceil_div(std::max<int64_t>(p->nbins, 1), kScanBlock);
-        HB_TRY(dev_alloc(p, (void**)&p->tmp_count, sizeof(int) * (p->nbins + 1), "bin counts"));
-        HB_TRY(dev_alloc(p, (void**)&p->tmp_ecnt, sizeof(int) * (p->nbins + 1), "subproblem counts"));
-        HB_TRY(dev_alloc(p, (void**)&p->tmp_eoff, sizeof(int) * (p->nbins + 1), "subproblem offsets"));
+        const int64_t nb = ceil_div(std::max<int64_t>(p->nbins_cap, 1), kScanBlock);
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_count, sizeof(int) * (p->nbins_cap + 1), "bin counts"));
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_ecnt, sizeof(int) * (p->nbins_cap + 1), "subproblem counts"));
+        HB_TRY(dev_alloc(p, (void**)&p->tmp_eoff, sizeof(int) * (p->nbins_cap + 1), "subproblem offsets"));
         HB_TRY(dev_alloc(p, (void**)&p->tmp_sums, sizeof(int) * nb, "scan sums"));
     }
     if (M > p->tmp_cap) {
@@ -1278,6 +1349,9 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             fa.err = p->d_err;
             fa.hw = p->kb.hw;
             fa.M = M;
+            fa.foff = nframes > 1 ? p->foff : nullptr;
+            fa.nfr = nframes;
+            fa.ntf = (int)g.ntf;
             k_fold_bin<<<(unsigned)ceil_div(M, 256), 256, 0, s>>>(fa);
             if ((st = check_launch("k_fold_bin")) != HB_OK) break;
         }
@@ -1295,6 +1369,8 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             if (p->maxp_auto) p->maxp = auto_subproblem(M, g);
             TileNbr tn;
             for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
+            tn.nfr = nframes;
+            tn.ntf = (int)g.ntf;
             k_tile_parts_count<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins, p->maxp, ecnt);
             if ((st = check_launch("k_tile_parts_count")) != HB_OK) break;
             if ((st = exclusive_scan_int(ecnt, eoff, p->nbins, s, p->tmp_sums)) != HB_OK) break;
@@ -1330,6 +1406,8 @@ int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const
             if (p->maxp_auto) p->maxp = auto_subproblem(M, g);
             TileNbr tn;
             for (int ax = 0; ax < 3; ++ax) tn.nb[ax] = g.nb[ax];
+            tn.nfr = nframes;
+            tn.ntf = (int)g.ntf;
             k_tile_extra_count<<<(unsigned)ceil_div(p->nbins, 256), 256, 0, s>>>(p->bin_start, tn, p->nbins,
                                                                                 p->maxp, ecnt);
             if ((st = check_launch("k_tile_extra_count")) != HB_OK) break;
@@ -1386,6 +1464,7 @@ static GridArgs grid_args(const NufftPlan* p) {
     for (int ax = 0; ax < 3; ++ax) a.su[ax] = p->su[ax];
     a.perm = p->perm;
     a.bin_start = p->bin_start;
+    a.foff = p->g.nfr > 1 ? p->foff : nullptr;
     a.inT = p->inT;
     a.grid = p->X;
     a.extra = p->extra;
@@ -1482,23 +1561,25 @@ static int type2_grid(NufftPlan* p, const float2* in, float2** G, cudaStream_t s
     const bool inv = p->sign > 0;
     const int64_t h0 = g.Nm[0] / 2, h1 = g.Nm[1] / 2, h2 = g.Nm[2] / 2;
     const int npass = 1 + (g.nf[1] > 1) + (g.nf[0] > 1);
+    const int64_t F = g.nfr;  // frames: one block of rows each in every pass
     float2* cur = (npass % 2 == 1) ? p->X : p->Y;
     float2* other = (cur == p->X) ? p->Y : p->X;
     {
-        OpModesIn op{in, cur, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm, (int64_t)g.nf[2] * C, C};
-        HB_TRY(launch_fft_pass(op, p->fl[2], g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv, 0, s,
+        OpModesIn op{in, cur, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm, (int64_t)g.nf[2] * C, C,
+                     g.Nm[0] * g.Nm[1], (int64_t)C * nm};
+        HB_TRY(launch_fft_pass(op, p->fl[2], F * g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv, 0, s,
                                "type2 axis2"));
     }
     if (g.nf[1] > 1) {
         const int64_t E = (int64_t)g.nf[2] * C;
         OpStrided op{cur, other, g.Nm[1] * E, E, (int64_t)g.nf[1] * E, E, 1.0f};
-        HB_TRY(launch_fft_pass(op, p->fl[1], g.Nm[0], E, (int)g.Nm[1], (int)-h1, g.nf[1], 0, inv, 0, s, "type2 axis1"));
+        HB_TRY(launch_fft_pass(op, p->fl[1], F * g.Nm[0], E, (int)g.Nm[1], (int)-h1, g.nf[1], 0, inv, 0, s, "type2 axis1"));
         std::swap(cur, other);
     }
     if (g.nf[0] > 1) {
         const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
-        OpStrided op{cur, other, 0, E, 0, E, 1.0f};
-        HB_TRY(launch_fft_pass(op, p->fl[0], 1, E, (int)g.Nm[0], (int)-h0, g.nf[0], 0, inv, 0, s, "type2 axis0"));
+        OpStrided op{cur, other, g.Nm[0] * E, E, (int64_t)g.nf[0] * E, E, 1.0f};
+        HB_TRY(launch_fft_pass(op, p->fl[0], F, E, (int)g.Nm[0], (int)-h0, g.nf[0], 0, inv, 0, s, "type2 axis0"));
         std::swap(cur, other);
     }
     *G = cur;
@@ -1532,25 +1613,26 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
             HB_TRY(dispatch_cc(spread_cc(g), p, a, s, true));
         float2* cur = p->X;
         float2* other = p->Y;
-        // axis 0: [nf0][nf1*nf2*C] -> [Nm0][...]
+        const int64_t F = g.nfr;  // frames: one block of rows each in every pass
+        // axis 0: [F][nf0][nf1*nf2*C] -> [F][Nm0][...]
         if (g.nf[0] > 1) {
             const int64_t E = (int64_t)g.nf[1] * g.nf[2] * C;
-            OpStrided op{cur, other, 0, E, 0, E, 1.0f};
-            HB_TRY(launch_fft_pass(op, p->fl[0], 1, E, g.nf[0], 0, (int)g.Nm[0], (int)-h0, inv, 0, s, "type1 axis0"));
+            OpStrided op{cur, other, (int64_t)g.nf[0] * E, E, g.Nm[0] * E, E, 1.0f};
+            HB_TRY(launch_fft_pass(op, p->fl[0], F, E, g.nf[0], 0, (int)g.Nm[0], (int)-h0, inv, 0, s, "type1 axis0"));
             std::swap(cur, other);
         }
-        // axis 1: [Nm0][nf1][nf2*C] -> [Nm0][Nm1][nf2*C]
+        // axis 1: [F Nm0][nf1][nf2*C] -> [F Nm0][Nm1][nf2*C]
         if (g.nf[1] > 1) {
             const int64_t E = (int64_t)g.nf[2] * C;
             OpStrided op{cur, other, (int64_t)g.nf[1] * E, E, g.Nm[1] * E, E, 1.0f};
-            HB_TRY(launch_fft_pass(op, p->fl[1], g.Nm[0], E, g.nf[1], 0, (int)g.Nm[1], (int)-h1, inv, 0, s, "type1 axis1"));
+            HB_TRY(launch_fft_pass(op, p->fl[1], F * g.Nm[0], E, g.nf[1], 0, (int)g.Nm[1], (int)-h1, inv, 0, s, "type1 axis1"));
             std::swap(cur, other);
         }
-        // axis 2 -> caller's modes with deapodisation
+        // axis 2 -> caller's modes [F][C][Nm..] with deapodisation
         {
             OpModesOut op{cur, out, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm,
-                          (int64_t)g.nf[2] * C, C};
-            HB_TRY(launch_fft_pass(op, p->fl[2], g.Nm[0] * g.Nm[1], C, g.nf[2], 0, (int)g.Nm[2], (int)-h2, inv, 0, s,
+                          (int64_t)g.nf[2] * C, C, g.Nm[0] * g.Nm[1], (int64_t)C * nm};
+            HB_TRY(launch_fft_pass(op, p->fl[2], F * g.Nm[0] * g.Nm[1], C, g.nf[2], 0, (int)g.Nm[2], (int)-h2, inv, 0, s,
                                    "type1 axis2"));
         }
         return HB_OK;
@@ -1681,6 +1763,8 @@ void plan_free(NufftPlan* p) {
     }
     if (p->X) cudaFree(p->X);
     if (p->Y) cudaFree(p->Y);
+    if (p->foff) cudaFree(p->foff);
+    p->foff = nullptr;
     if (p->perm) cudaFree(p->perm);
     if (p->inT) cudaFree(p->inT);
     if (p->bin_start) cudaFree(p->bin_start);

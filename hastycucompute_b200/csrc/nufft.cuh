@@ -26,7 +26,13 @@ struct GridGeom {
     int T[3];         // tile edge per axis
     int nb[3];        // tiles (bins) per axis
     float scale[3];   // nf / (2 pi), float32
-    int64_t M;        // points
+    int64_t M;        // points (all frames)
+    // frames: independent trajectories of one plan. Frame f owns fine grid block f (fgrid values),
+    // bins f * ntf .. f * ntf + ntf - 1 and the points foff[f] .. foff[f+1] - 1 (caller and sorted
+    // order alike: the bins are frame-major, so sorting keeps every frame's points together).
+    int nfr;          // frames (1: a single trajectory)
+    int64_t ntf;      // tiles (bins) per frame
+    int64_t fgrid;    // fine grid values per frame (cells x C)
 };
 
 struct NufftPlan {
@@ -54,6 +60,12 @@ struct NufftPlan {
     int64_t extra_cap = 0;
     int* d_err = nullptr;
     bool pts_set = false;
+    // frames: grids are allocated for frames_cap frames; foff holds the current frames' point
+    // offsets (device, g.nfr + 1 entries)
+    int frames_cap = 1;
+    int* foff = nullptr;
+    int64_t foff_cap = 0;
+    int64_t nbins_cap = 0;  // entries of the per-bin scratch (bin counts, subproblem counts)
     // setpts scratch, kept by the plan so that re-pointing it allocates nothing: per point
     // (grown with M) and per bin (allocated at the first setpts)
     float* tmp_u[3] = {nullptr, nullptr, nullptr};
@@ -101,12 +113,34 @@ struct GridArgs {
     const float2* inT;  // spread input [M][C], transforms interleaved, caller's point order
     float2* grid;       // [nf0][nf1][nf2][C]
     float2* out;        // interp output [C][M]
+    const int* foff;    // frame point offsets [nfr + 1] (nullptr with one frame)
     const int2* extra;
     int maxp;
     KbPoly kb;
 };
 
 constexpr int kCoefFloats = kMaxWidth * (kMaxDeg + 1);
+
+#ifdef __CUDACC__
+// Frame of point s (caller or sorted index: both keep every frame's points contiguous). Empty
+// frames are skipped: the last f with foff[f] <= s.
+__device__ __forceinline__ int frame_of_point(const int* foff, int nfr, int64_t s) {
+    if (nfr <= 1) return 0;
+    int lo = 0, hi = nfr;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (foff[mid] <= s) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+// Tile over all frames (frame-major) -> its frame; `tile` becomes the frame's own tile index.
+__device__ __forceinline__ int split_frame_tile(const GridGeom& g, int& tile) {
+    if (g.nfr <= 1) return 0;
+    const int fr = (int)(tile / g.ntf);
+    tile -= fr * (int)g.ntf;
+    return fr;
+}
+#endif
 
 // Type-1 spreading with the transforms on the lanes (spread_lc.cuh; instances in
 // spread_lc{8,16,32}.cu) for plans with p->lc set, by transform chunk.
@@ -117,6 +151,10 @@ int spread_lc_cc32(const NufftPlan* p, const GridArgs& a, cudaStream_t s);
 int plan_make(NufftPlan* p, int type, int dim, const int64_t* nmodes, int sign, int ntransf, float tol,
               int width, double upsampfac, int method);
 int plan_setpts(NufftPlan* p, int64_t M, const float* c0, const float* c1, const float* c2, cudaStream_t s);
+// Points of nframes frames at once: frame f has npts[f] (host) points, stored one frame after the
+// other in c0 / c1 / c2. Grows the plan's grids to nframes frames when needed.
+int plan_setpts_frames(NufftPlan* p, int nframes, const int64_t* npts, const float* c0, const float* c1,
+                       const float* c2, cudaStream_t s);
 int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s);
 int plan_coord_grad(NufftPlan* p, const float2* modes, const float2* h, float* grad, cudaStream_t s);
 int plan_set_spread_tuning(NufftPlan* p, int maxp, int bz, int by, int bx);

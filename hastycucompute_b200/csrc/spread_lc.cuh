@@ -119,7 +119,11 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
     const int grp = lane / CC, coil = lane % CC;
 
     const int4 job = parts ? parts[blockIdx.x] : make_int4((int)blockIdx.x, 0, 1, 0);
-    const int tile = job.x, part = job.y, K = job.z;
+    int tile = job.x;
+    const int part = job.y, K = job.z;
+    const int fr = split_frame_tile(g, tile);
+    const int fbin = fr * (int)g.ntf;
+    float2* const gridf = a.grid + fr * g.fgrid;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int org0 = tz * S::T0, org1 = ty * S::T1, org2 = tx * S::T2;
     const int nf1 = g.nf[1], nf2 = g.nf[2];
@@ -140,8 +144,8 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
             const int bz = (tz - dz + g.nb[0]) % g.nb[0], by = (ty - dy + g.nb[1]) % g.nb[1];
             const int bx = (tx - dx + g.nb[2]) % g.nb[2];
             const int bin = (bz * g.nb[1] + by) * g.nb[2] + bx;
-            st = a.bin_start[bin];
-            cnt = a.bin_start[bin + 1] - st;
+            st = a.bin_start[fbin + bin];
+            cnt = a.bin_start[fbin + bin + 1] - st;
         }
         int incl = cnt;
 #pragma unroll
@@ -173,7 +177,7 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
                 const int r = i / rowf4, c4 = i - r * rowf4;
                 const int zz = r / S::T1, yy = r - zz * S::T1;
                 float4* dst = reinterpret_cast<float4*>(
-                    a.grid + (((int64_t)(org0 + zz) * nf1 + (org1 + yy)) * nf2 + org2) * g.C);
+                    gridf + (((int64_t)(org0 + zz) * nf1 + (org1 + yy)) * nf2 + org2) * g.C);
                 dst[c4] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             return;
@@ -329,7 +333,7 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
         for (int r = 0; r < 4; ++r) {
             const int z = z0 + (D3 ? (r >> 1) : 0), y = y0g + (D3 ? (r & 1) : r);
             float2* row = parts ? dst + ((int64_t)(z * S::T1 + y) * S::T2 + x0) * g.C + cc0 + coil
-                                : a.grid + (((int64_t)(org0 + z) * nf1 + (org1 + y)) * nf2 + org2 + x0) * g.C + cc0 + coil;
+                                : gridf + (((int64_t)(org0 + z) * nf1 + (org1 + y)) * nf2 + org2 + x0) * g.C + cc0 + coil;
             if (coil_ok) {
 #pragma unroll
                 for (int x = 0; x < 8; ++x) row[(int64_t)x * g.C] = make_float2(ar[r][x], ai[r][x]);
@@ -347,7 +351,9 @@ __global__ void __launch_bounds__(256) k_spread_lc_reduce(const GridArgs a, cons
     using S = LcShape<32, D3>;
     const GridGeom& g = a.g;
     const int4 e = parts[blockIdx.x];
-    const int tile = e.x;
+    int tile = e.x;
+    const int fr = split_frame_tile(g, tile);
+    float2* const gridf = a.grid + fr * g.fgrid;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int org0 = tz * S::T0, org1 = ty * S::T1, org2 = tx * S::T2;
     const int64_t E = (int64_t)S::CELLS * g.C;
@@ -363,7 +369,7 @@ __global__ void __launch_bounds__(256) k_spread_lc_reduce(const GridArgs a, cons
         const int64_t cell = i / g.C;
         const int c = (int)(i - cell * g.C);
         const int x = (int)(cell % S::T2), y = (int)((cell / S::T2) % S::T1), z = (int)(cell / (S::T2 * S::T1));
-        a.grid[(((int64_t)(org0 + z) * g.nf[1] + (org1 + y)) * g.nf[2] + org2 + x) * g.C + c] = sum;
+        gridf[(((int64_t)(org0 + z) * g.nf[1] + (org1 + y)) * g.nf[2] + org2 + x) * g.C + c] = sum;
     }
 }
 

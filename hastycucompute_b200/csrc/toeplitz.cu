@@ -191,13 +191,17 @@ struct OpToepMid {
     int Lk;
     __device__ __forceinline__ float2 load(int64_t, int l, int64_t e) const { return buf[(int64_t)l * E + e]; }
     __device__ __forceinline__ const float2* sample_ptr(int64_t, int l, int64_t e) const { return buf + (int64_t)l * E + e; }
-    __device__ __forceinline__ int64_t kcol(int64_t e) const { return e / B; }
+    // kernel column of column e: a 32-bit division whenever the operands fit (every workspace
+    // this library sizes), the 64-bit one otherwise
+    __device__ __forceinline__ int64_t kcol(int64_t e) const {
+        return ((uint64_t)e | (uint64_t)B) <= 0xffffffffull ? (int64_t)((uint32_t)e / (uint32_t)B) : e / B;
+    }
     __device__ __forceinline__ const float2* kptr(int64_t kc) const { return kt + kc * Lk; }
     __device__ __forceinline__ const float2* srow(int64_t, int64_t) const { return nullptr; }
     __device__ __forceinline__ float2 product_s(float2 v, float2) const { return v; }
     __device__ __forceinline__ int64_t group(int64_t) const { return 0; }
     __device__ __forceinline__ int ngroups() const { return 1; }
-    __device__ __forceinline__ float2 kval(int64_t, int pos, int64_t e) const { return kt[(e / B) * Lk + pos]; }
+    __device__ __forceinline__ float2 kval(int64_t, int pos, int64_t e) const { return kt[kcol(e) * Lk + pos]; }
     __device__ __forceinline__ void store(int64_t, int o, int64_t e, float2 v) const { buf[(int64_t)o * E + e] = v; }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
     __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
@@ -656,10 +660,25 @@ int transform_toeplitz_kernel(int dim, const int64_t* kshape, const void* kin, v
     return check_launch("transform_toeplitz_kernel");
 }
 
+int toeplitz_kernel_frames(int dim, const int64_t* kshape, int nframes, const int64_t* npts, const float* c0,
+                           const float* c1, const float* c2, const void* nudata, void* kout, int width, cudaStream_t s);
+
 int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, const float* c1, const float* c2,
                     const void* nudata, void* kout, int width, cudaStream_t s) {
+    return toeplitz_kernel_frames(dim, kshape, 1, &M, c0, c1, c2, nudata, kout, width, s);
+}
+
+// The kernels of nframes frames: one frame-batched type-1 NUFFT over every frame's points, then
+// the zero-padding FFT passes over all frames' rows at once. kout is [nframes][2N..].
+int toeplitz_kernel_frames(int dim, const int64_t* kshape, int nframes, const int64_t* npts, const float* c0,
+                           const float* c1, const float* c2, const void* nudata, void* kout, int width, cudaStream_t s) {
     HB_REQUIRE(dim >= 2 && dim <= 3, HB_ERR_INVALID_ARG, "Toeplitz kernel must be 2-D or 3-D");
-    HB_REQUIRE(kshape && nudata && kout, HB_ERR_INVALID_ARG, "null argument");
+    HB_REQUIRE(kshape && npts && kout, HB_ERR_INVALID_ARG, "null argument");
+    HB_REQUIRE(nframes >= 1, HB_ERR_INVALID_ARG, "nframes must be >= 1");
+    int64_t Mtot = 0;
+    for (int f = 0; f < nframes; ++f) Mtot += npts[f] > 0 ? npts[f] : 0;
+    HB_REQUIRE(nudata || Mtot == 0, HB_ERR_INVALID_ARG, "null argument");
+    const int64_t F = nframes;
     int64_t nm[3], L[3] = {1, 1, 1}, Nimg = 1;
     for (int i = 0; i < dim; ++i) {
         HB_REQUIRE(kshape[i] >= 4 && kshape[i] % 2 == 0, HB_ERR_SHAPE, "kernel dimensions must be even (2N)");
@@ -681,17 +700,17 @@ int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, 
         return st;
     }
     const int64_t r0 = L[0] > 1 ? L[0] - 1 : 1, r1 = L[1] - 1, r2 = L[2] - 1;
-    const size_t nred = (size_t)r0 * r1 * r2;
+    const size_t nred = (size_t)F * r0 * r1 * r2;
     cudaError_t e = cudaMalloc(&red, sizeof(float2) * nred);
-    if (e == cudaSuccess) e = cudaMalloc(&b1, sizeof(float2) * (size_t)r0 * r1 * L[2]);
-    if (e == cudaSuccess) e = cudaMalloc(&b2, sizeof(float2) * (size_t)r0 * L[1] * L[2]);
+    if (e == cudaSuccess) e = cudaMalloc(&b1, sizeof(float2) * (size_t)F * r0 * r1 * L[2]);
+    if (e == cudaSuccess) e = cudaMalloc(&b2, sizeof(float2) * (size_t)F * r0 * L[1] * L[2]);
     if (e != cudaSuccess) {
         cleanup();
         set_error(std::string("toeplitz_kernel temporaries: ") + cudaGetErrorString(e));
         return HB_ERR_ALLOC;
     }
     do {
-        if ((st = plan_setpts(&plan, M, c0, c1, c2, s)) != HB_OK) break;
+        if ((st = plan_setpts_frames(&plan, nframes, npts, c0, c1, c2, s)) != HB_OK) break;
         if ((st = plan_execute(&plan, (const float2*)nudata, red, s)) != HB_OK) break;
         FftLen f0, f1, f2;
         if ((st = get_len((int)L[2], &f2)) != HB_OK) break;
@@ -699,23 +718,26 @@ int toeplitz_kernel(int dim, const int64_t* kshape, int64_t M, const float* c0, 
         if (dim == 3 && (st = get_len((int)L[0], &f0)) != HB_OK) break;
         const float scale = (float)(1.0 / (double)Nimg);
         float2* K = (float2*)kout;
-        // axis 2: [r0*r1][r2] -> b1 [r0*r1][L2]
+        // axis 2: [F r0 r1][r2] -> b1 [F r0 r1][L2]
         {
             OpStrided op{red, b1, r2, 1, L[2], 1, 1.0f};
-            if ((st = launch_fft_pass(op, f2, r0 * r1, 1, (int)r2, 0, (int)L[2], 0, 0, 0, s, "toeplitz_kernel axis2")) != HB_OK)
+            if ((st = launch_fft_pass(op, f2, F * r0 * r1, 1, (int)r2, 0, (int)L[2], 0, 0, 0, s, "toeplitz_kernel axis2")) !=
+                HB_OK)
                 break;
         }
-        // axis 1: [r0][r1][L2] -> [r0][L1][L2]
+        // axis 1: [F r0][r1][L2] -> [F r0][L1][L2]
         {
             float2* dst = dim == 3 ? b2 : K;
             OpStrided op{b1, dst, r1 * L[2], L[2], L[1] * L[2], L[2], dim == 3 ? 1.0f : scale};
-            if ((st = launch_fft_pass(op, f1, r0, L[2], (int)r1, 0, (int)L[1], 0, 0, 0, s, "toeplitz_kernel axis1")) != HB_OK)
+            if ((st = launch_fft_pass(op, f1, F * r0, L[2], (int)r1, 0, (int)L[1], 0, 0, 0, s, "toeplitz_kernel axis1")) !=
+                HB_OK)
                 break;
         }
+        // axis 0: [F][r0][L1 L2] -> [F][L0][L1 L2]
         if (dim == 3) {
             const int64_t E = L[1] * L[2];
-            OpStrided op{b2, K, 0, E, 0, E, scale};
-            if ((st = launch_fft_pass(op, f0, 1, E, (int)r0, 0, (int)L[0], 0, 0, 0, s, "toeplitz_kernel axis0")) != HB_OK)
+            OpStrided op{b2, K, r0 * E, E, L[0] * E, E, scale};
+            if ((st = launch_fft_pass(op, f0, F, E, (int)r0, 0, (int)L[0], 0, 0, 0, s, "toeplitz_kernel axis0")) != HB_OK)
                 break;
         }
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {

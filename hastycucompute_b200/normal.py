@@ -103,6 +103,47 @@ class SenseOp:
         return self.adjoint(self.forward(x))
 
 
+class BatchedSenseOp:
+    """Plain SENSE A / A^H over frames with their own (ragged) trajectories and shared coil maps,
+    one frame-batched NUFFT plan pair: every pass of the type 2 and type 1 covers all frames' points
+    in one launch (the per-frame plan loop of hasty_python/right_precond_test.py:48-73 and
+    simul_op.py:39-91 replaced). Images are [F, N..]; non-uniform data [C, M] with the frames'
+    points back to back along M."""
+
+    def __init__(self, frame_coords, smaps: torch.Tensor, kernel_width: int = 0, tol: float = 1e-5,
+                 scale: float = 1.0, spread_tuning: Optional[dict] = None):
+        self.smaps = smaps.contiguous()
+        self.shape = tuple(smaps.shape[1:])
+        self.ncoils = smaps.shape[0]
+        self.scale = float(scale)
+        opts = NufftOpts(nmodes=self.shape, ntransf=self.ncoils, tol=tol, kernel_width=kernel_width)
+        self.fwd = NufftPlan(NufftType.TYPE_2, opts)
+        self.adj = NufftPlan(NufftType.TYPE_1, opts)
+        if spread_tuning is not None:
+            from .autotune import apply
+            apply(self.adj, spread_tuning)
+        self.setpts(frame_coords)
+
+    def setpts(self, frame_coords) -> None:
+        self.fwd.setpts_frames(frame_coords)
+        self.adj.setpts_frames(frame_coords)
+        self.nframes = len(frame_coords)
+        self.frame_points = self.fwd.frame_points
+        self.M = self.fwd.M
+
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        y = self.fwd((self.smaps.unsqueeze(0) * x.unsqueeze(1)).contiguous())
+        return y * self.scale if self.scale != 1.0 else y
+
+    def adjoint(self, y: torch.Tensor) -> torch.Tensor:
+        img = self.adj(y.contiguous())
+        out = (self.smaps.conj().unsqueeze(0) * img).sum(1)
+        return out * self.scale if self.scale != 1.0 else out
+
+    def normal(self, x: torch.Tensor) -> torch.Tensor:
+        return self.adjoint(self.forward(x))
+
+
 class BatchedNormalOp:
     """Frames with their own Toeplitz kernels and shared coil maps in one apply:
     out[f] = sum_c conj(S_c) T_f(S_c x[f]) for x [F, N..]. Every pass runs all F x C columns in
@@ -140,13 +181,23 @@ class BatchedNormalOp:
     __call__ = apply
 
 
-def build_toeplitz_kernels(frame_coords, shape, weights=None, kernel_width: int = 0) -> torch.Tensor:
-    """Straight kernels [F, 2N..] for frames with their own (ragged) trajectories."""
-    ks = []
-    for f, coords in enumerate(frame_coords):
-        w = None if weights is None else weights[f]
-        ks.append(build_toeplitz_kernel(coords, shape, w, kernel_width=kernel_width))
-    return torch.stack(ks)
+def build_toeplitz_kernels(frame_coords, shape, weights=None, kernel_width: int = 0,
+                           max_bytes: int = 16 << 30) -> torch.Tensor:
+    """Straight kernels [F, 2N..] for frames with their own (ragged) trajectories: frame-batched
+    builds (one type-1 NUFFT launch per pass over a group of frames), in groups whose temporary
+    grids stay under about ``max_bytes``."""
+    from .toeplitz import toeplitz_kernels_frames
+    F = len(frame_coords)
+    dev = frame_coords[0][0].device
+    kshape = tuple(2 * int(s) for s in shape)
+    per_frame = 8 * 2 * (2 ** len(shape)) * int(torch.tensor(kshape).prod().item())  # fine grid + pass buffers
+    group = max(1, min(F, int(max_bytes) // max(per_frame, 1)))
+    out = torch.empty((F, *kshape), dtype=torch.complex64, device=dev)
+    for f0 in range(0, F, group):
+        f1 = min(F, f0 + group)
+        w = None if weights is None else [weights[f] for f in range(f0, f1)]
+        toeplitz_kernels_frames([frame_coords[f] for f in range(f0, f1)], out[f0:f1], w, kernel_width=kernel_width)
+    return out
 
 
 class NormalTT2Op:

@@ -93,6 +93,8 @@ class NufftPlan:
         self.ntransf = int(opts.ntransf)
         self.device = torch.device("cuda", opts.device_idx if opts.device_idx is not None else torch.cuda.current_device())
         self.M = None
+        self.nframes = None  # set by setpts_frames: execute then takes / gives frame-stacked modes
+        self.frame_points = None
         self._coords = None
         with torch.cuda.device(self.device):
             _lib.call("hb_nufft_makeplan", int(self.type), self.dim, _lib.i64_array(self.nmodes),
@@ -118,7 +120,44 @@ class NufftPlan:
         with torch.cuda.device(self.device):
             _lib.call("hb_nufft_setpts", self._h, int(M), cp[0], cp[1], cp[2], stream_ptr(self.device))
         self.M = int(M)
+        self.nframes = None
+        self.frame_points = None
         self._coords = tuple(coords)
+
+    def setpts_frames(self, frame_coords: Sequence[Sequence[torch.Tensor]]) -> None:
+        """Points of several frames (each its own trajectory, any number of points, zero allowed)
+        in one plan: one bin sort now and one launch per pass at every execute, in place of one
+        plan execute per frame (the per-frame loops of hasty_python/simul_op.py:39-91 and
+        right_precond_test.py:48-73). After it, execute takes / gives
+
+            type 1: input [ntransf, M] -> output [nframes, ntransf, *nmodes]
+            type 2: input [nframes, ntransf, *nmodes] -> output [ntransf, M]
+
+        with M the total point count and the frames' points back to back along M."""
+        F = len(frame_coords)
+        if F < 1:
+            raise ValueError("need at least one frame")
+        counts = []
+        for f, coords in enumerate(frame_coords):
+            if len(coords) != self.dim:
+                raise ValueError(f"frame {f}: expected {self.dim} coordinate arrays")
+            m = coords[0].shape[0]
+            for i, c in enumerate(coords):
+                check_tensor(c, f"frame {f} coords[{i}]", torch.float32, (m,), self.device)
+            counts.append(int(m))
+        cat = [torch.cat([fc[i] for fc in frame_coords]).contiguous() for i in range(self.dim)]
+        cp = [ptr(c) for c in cat] + [C.c_void_p(None)] * (3 - self.dim)
+        with torch.cuda.device(self.device):
+            _lib.call("hb_nufft_setpts_frames", self._h, F, _lib.i64_array(counts), cp[0], cp[1], cp[2],
+                      stream_ptr(self.device))
+        self.M = int(sum(counts))
+        self.nframes = F
+        self.frame_points = tuple(counts)
+        self._coords = tuple(cat)
+
+    def _mode_shape(self) -> tuple:
+        base = (self.ntransf, *self.nmodes)
+        return base if self.nframes is None else (self.nframes, *base)
 
     def execute(self, input: torch.Tensor, output: torch.Tensor) -> torch.Tensor:
         """nufft_plan::execute (nufft.cppm:205-250).
@@ -130,9 +169,9 @@ class NufftPlan:
             raise RuntimeError("execute called before setpts")
         if self.type == NufftType.TYPE_1:
             check_tensor(input, "input", torch.complex64, (self.ntransf, self.M), self.device)
-            check_tensor(output, "output", torch.complex64, (self.ntransf, *self.nmodes), self.device)
+            check_tensor(output, "output", torch.complex64, self._mode_shape(), self.device)
         else:
-            check_tensor(input, "input", torch.complex64, (self.ntransf, *self.nmodes), self.device)
+            check_tensor(input, "input", torch.complex64, self._mode_shape(), self.device)
             check_tensor(output, "output", torch.complex64, (self.ntransf, self.M), self.device)
         with torch.cuda.device(self.device):
             _lib.call("hb_nufft_execute", self._h, ptr(input), ptr(output), stream_ptr(self.device))
@@ -195,7 +234,7 @@ class NufftPlan:
 
     def __call__(self, input: torch.Tensor) -> torch.Tensor:
         if self.type == NufftType.TYPE_1:
-            out = torch.empty((self.ntransf, *self.nmodes), dtype=torch.complex64, device=self.device)
+            out = torch.empty(self._mode_shape(), dtype=torch.complex64, device=self.device)
         else:
             out = torch.empty((self.ntransf, self.M), dtype=torch.complex64, device=self.device)
         return self.execute(input, out)

@@ -62,6 +62,44 @@ def toeplitz_kernel(coords: Sequence[torch.Tensor], kernel: torch.Tensor, nudata
     return kernel
 
 
+def toeplitz_kernels_frames(frame_coords: Sequence[Sequence[torch.Tensor]], kernels: torch.Tensor,
+                            frame_nudata: Optional[Sequence[torch.Tensor]] = None, kernel_width: int = 0) -> torch.Tensor:
+    """toeplitz_kernel for F frames in one call: fills ``kernels`` ([F, 2N..], complex64). Frame f
+    has its own points ``frame_coords[f]`` (any count, zero allowed) and weights
+    ``frame_nudata[f]`` ([M_f] or [1, M_f]; ones when None). One frame-batched type-1 NUFFT and
+    one launch per FFT pass serve all frames, in place of one plan per frame."""
+    F = kernels.shape[0]
+    dim = kernels.dim() - 1
+    if dim not in (2, 3):
+        raise ValueError("kernels must be [F, 2N..] with 2-D or 3-D frames")
+    if len(frame_coords) != F:
+        raise ValueError("one coordinate set per frame")
+    check_tensor(kernels, "kernels", torch.complex64, None, kernels.device)
+    dev = kernels.device
+    counts, nds = [], []
+    for f, coords in enumerate(frame_coords):
+        if len(coords) != dim:
+            raise ValueError(f"frame {f}: expected {dim} coordinate arrays")
+        m = coords[0].shape[0]
+        for i, c in enumerate(coords):
+            check_tensor(c, f"frame {f} coords[{i}]", torch.float32, (m,), dev)
+        if frame_nudata is None:
+            nds.append(torch.ones(m, dtype=torch.complex64, device=dev))
+        else:
+            nd = frame_nudata[f].reshape(-1).to(torch.complex64)
+            if nd.shape[0] != m:
+                raise ValueError(f"frame {f}: nudata length differs from the coordinates")
+            nds.append(nd)
+        counts.append(int(m))
+    cat = [torch.cat([fc[i] for fc in frame_coords]).contiguous() for i in range(dim)]
+    nd = torch.cat(nds).contiguous()
+    cp = [ptr(c) for c in cat] + [C.c_void_p(None)] * (3 - dim)
+    with torch.cuda.device(dev):
+        _lib.call("hb_toeplitz_kernels_frames", dim, _lib.i64_array(kernels.shape[1:]), F, _lib.i64_array(counts),
+                  cp[0], cp[1], cp[2], ptr(nd), ptr(kernels), int(kernel_width), stream_ptr(dev))
+    return kernels
+
+
 def transform_toeplitz_kernel(kernel: torch.Tensor) -> torch.Tensor:
     """transform_toeplitz_kernel (toeplitz.cppm:510-609): returns the kernel in the layout the
     fused multiplication reads (a new tensor, same element count)."""

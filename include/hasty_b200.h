@@ -91,6 +91,19 @@ int hb_nufft_makeplan(int type, int dim, const int64_t* nmodes, int sign, int nt
 int hb_nufft_setpts(hb_nufft_plan plan, int64_t M, const float* coord0, const float* coord1,
                     const float* coord2, void* stream);
 
+/* Frames in one plan: replaces the per-frame loop of plans (one setpts + execute per frame's
+ * trajectory, hasty_python/simul_op.py:39-91, right_precond_test.py:48-73) with one bin sort
+ * and one launch per pass over every frame's points. Frame f has npts[f] points (host array of
+ * nframes counts, zeros allowed); the device coordinate arrays hold the frames one after the
+ * other (M = sum npts). Grows the plan's grids to nframes frames on first use. After it, execute
+ * reads and writes (M_f = npts[f], rows of all frames back to back):
+ *   type 1: in = c64 [ntransf, M],  out = c64 [nframes, ntransf, N0, ..];
+ *   type 2: in = c64 [nframes, ntransf, N0, ..], out = c64 [ntransf, M].
+ * hb_nufft_setpts is this call with one frame. */
+int hb_nufft_setpts_frames(hb_nufft_plan plan, int nframes, const int64_t* npts,
+                           const float* coord0, const float* coord1, const float* coord2,
+                           void* stream);
+
 /* nufft_plan::execute, nufft.cppm:205-250.
  *   type 1: in = c64 [ntransf, M] nonuniform data, out = c64 [ntransf, N0, ..] modes;
  *   type 2: in = c64 [ntransf, N0, ..] modes,      out = c64 [ntransf, M].
@@ -160,6 +173,18 @@ int hb_nufft_get_info(hb_nufft_plan plan, int64_t* fine_out3, int* width_out,
 int hb_toeplitz_kernel(int dim, const int64_t* kernel_shape, int64_t M, const float* coord0,
                        const float* coord1, const float* coord2, const void* nudata,
                        void* kernel_out, int kernel_width, void* stream);
+
+/* toeplitz_kernel for nframes frames in one call (the per-frame kernel builds of
+ * hasty_python/simul_op.py:39-91 and right_precond_test.py:48-73, there one cufinufft plan and
+ * toeplitz_kernel call per frame): one frame-batched type-1 NUFFT over all frames' points
+ * (frame f has npts[f] points, frames back to back in coord* and nudata, as for
+ * hb_nufft_setpts_frames) and one launch per FFT pass over all frames. kernel_out is
+ * c64 [nframes, 2N0, ..]. Allocates and frees its temporaries (about nframes times the
+ * one-frame call's). */
+int hb_toeplitz_kernels_frames(int dim, const int64_t* kernel_shape, int nframes,
+                               const int64_t* npts, const float* coord0, const float* coord1,
+                               const float* coord2, const void* nudata, void* kernel_out,
+                               int kernel_width, void* stream);
 
 /* transform_toeplitz_kernel, cpp/corelib/lib/fft/toeplitz.cppm:510-609: re-lays the
  * straight kernel ([2N..] c64, from hb_toeplitz_kernel) into the layout
