@@ -356,8 +356,10 @@ __global__ void __launch_bounds__(kPassThreads) pass_kernel(const Op op, const P
         eb_begin = 0;
         eb_end = c.n_eb;
     } else {
-        ab = blockIdx.x / c.n_eb;
-        eb_begin = blockIdx.x % c.n_eb;
+        const unsigned neb = (unsigned)c.n_eb;  // grid < 2^31 blocks: a 32-bit split
+        const unsigned q = blockIdx.x / neb;
+        ab = q;
+        eb_begin = blockIdx.x - q * neb;
         eb_end = eb_begin + 1;
     }
     const int64_t a0 = ab * c.A_blk;

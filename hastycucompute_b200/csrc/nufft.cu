@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
 // Lanes of a warp map to (point slot, transform). Each lane keeps its point's first cells and tap
 // weights in registers, so the W^d gathers of a point are independent loads the compiler can
 // keep in flight together.
-template <int CC, int W>
+template <int CC, int W, bool FR>
 __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
     extern __shared__ float sm[];
     constexpr int NS = 32 / CC;
@@ -778,7 +778,8 @@ __global__ void __launch_bounds__(kGridThreads) k_interp_w(const GridArgs a) {
                 wx[d] = wts[2 * kMaxWidth + d];
             }
             const int pj = a.perm[s];
-            const float2* const gridf = a.grid + frame_of_point(a.foff, g.nfr, s) * g.fgrid;
+            // frames (FR): the grid block of the point's frame; one frame reads a.grid itself
+            const float2* const gridf = FR ? a.grid + frame_of_point(a.foff, g.nfr, s) * g.fgrid : a.grid;
             const unsigned rowstride = (unsigned)nf2 * (unsigned)g.C;
             // Common case: the footprint wraps neither along axis 2 nor axis 1 and the lanes hold
             // all C transforms, so a tap's column stride is the compile-time CC: one row pointer,
@@ -1008,11 +1009,19 @@ struct OpModesIn {
     const float* d2;
     int64_t N1, N2, nm;  // modes of axis 1, 2; modes per transform
     int64_t d_a, d_l;
-    int64_t rows_f, fstride;  // rows (N0 N1) and mode values (C nm) per frame
+    int64_t rows_f, fstride;  // frames: rows (N0 N1) and mode values (C nm) per frame; rows_f 0: one frame
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const {
-        const int64_t fr = a / rows_f, al = a - fr * rows_f;
-        const float sc = d0[al / N1] * d1[al % N1] * d2[l];
-        return cscale(f[fr * fstride + e * nm + al * N2 + l], sc);
+        // row a -> (frame, row of the frame) -> (mode 0, mode 1); 32-bit: F N0 N1 < 2^32 (setpts)
+        uint32_t al = (uint32_t)a;
+        int64_t fo = 0;
+        if (rows_f) {
+            const uint32_t fr = al / (uint32_t)rows_f;
+            al -= fr * (uint32_t)rows_f;
+            fo = (int64_t)fr * fstride;
+        }
+        const uint32_t i0 = al / (uint32_t)N1, i1 = al - i0 * (uint32_t)N1;
+        const float sc = d0[i0] * d1[i1] * d2[l];
+        return cscale(f[fo + e * nm + (int64_t)al * N2 + l], sc);
     }
     __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
@@ -1047,7 +1056,7 @@ struct OpModesOut {
     const float* d2;
     int64_t N1, N2, nm;
     int64_t s_a, s_l;
-    int64_t rows_f, fstride;  // rows (N0 N1) and mode values (C nm) per frame
+    int64_t rows_f, fstride;  // frames: rows (N0 N1) and mode values (C nm) per frame; rows_f 0: one frame
     __device__ __forceinline__ float2 load(int64_t a, int l, int64_t e) const { return src[a * s_a + (int64_t)l * s_l + e]; }
     __device__ __forceinline__ int64_t kcol(int64_t) const { return 0; }
     __device__ __forceinline__ const float2* kptr(int64_t) const { return nullptr; }
@@ -1057,9 +1066,16 @@ struct OpModesOut {
     __device__ __forceinline__ int ngroups() const { return 1; }
     __device__ __forceinline__ float2 kval(int64_t, int, int64_t) const { return make_float2(0.f, 0.f); }
     __device__ __forceinline__ void store(int64_t a, int o, int64_t e, float2 v) const {
-        const int64_t fr = a / rows_f, al = a - fr * rows_f;
-        const float sc = d0[al / N1] * d1[al % N1] * d2[o];
-        f[fr * fstride + e * nm + al * N2 + o] = cscale(v, sc);
+        uint32_t al = (uint32_t)a;
+        int64_t fo = 0;
+        if (rows_f) {
+            const uint32_t fr = al / (uint32_t)rows_f;
+            al -= fr * (uint32_t)rows_f;
+            fo = (int64_t)fr * fstride;
+        }
+        const uint32_t i0 = al / (uint32_t)N1, i1 = al - i0 * (uint32_t)N1;
+        const float sc = d0[i0] * d1[i1] * d2[o];
+        f[fo + e * nm + (int64_t)al * N2 + o] = cscale(v, sc);
     }
     __device__ __forceinline__ float2 product(int64_t, int, int64_t, float2 v) const { return v; }
     __device__ __forceinline__ void write_row(int64_t, int, int, float2) const {}
@@ -1243,6 +1259,7 @@ int plan_setpts_frames(NufftPlan* p, int nframes, const int64_t* npts, const flo
         hoff[(size_t)f + 1] = (int)M;
     }
     HB_REQUIRE((int64_t)p->g.ntf * nframes < (int64_t)0x7fffffff, HB_ERR_INVALID_ARG, "too many frames for the grid");
+    HB_REQUIRE(p->g.Nm[0] * p->g.Nm[1] * nframes < ((int64_t)1 << 32), HB_ERR_INVALID_ARG, "too many frames for the modes");
     // grids and per-bin scratch for nframes frames (grown, never shrunk)
     if (nframes > p->frames_cap) {
         if (p->X) cudaFree(p->X);
@@ -1515,9 +1532,14 @@ static int launch_interp_w(const NufftPlan* p, const GridArgs& a, cudaStream_t s
     int64_t blocks = ceil_div(std::max<int64_t>(p->g.M, 1), per_block);
     blocks = std::min<int64_t>(blocks, (int64_t)kNumSMs * 64);
     const size_t smem = sizeof(float) * (kCoefFloats + (size_t)kGridWarps * (32 / CC) * kSlotFloats);
-    HB_CUDA(cudaFuncSetAttribute(k_interp_w<CC, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     TimedSection ts("interp", s);
-    k_interp_w<CC, W><<<(unsigned)blocks, kGridThreads, smem, s>>>(a);
+    if (a.foff) {
+        HB_CUDA(cudaFuncSetAttribute(k_interp_w<CC, W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_interp_w<CC, W, true><<<(unsigned)blocks, kGridThreads, smem, s>>>(a);
+    } else {
+        HB_CUDA(cudaFuncSetAttribute(k_interp_w<CC, W, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_interp_w<CC, W, false><<<(unsigned)blocks, kGridThreads, smem, s>>>(a);
+    }
     return check_launch("k_interp");
 }
 
@@ -1566,7 +1588,7 @@ static int type2_grid(NufftPlan* p, const float2* in, float2** G, cudaStream_t s
     float2* other = (cur == p->X) ? p->Y : p->X;
     {
         OpModesIn op{in, cur, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm, (int64_t)g.nf[2] * C, C,
-                     g.Nm[0] * g.Nm[1], (int64_t)C * nm};
+                     F > 1 ? g.Nm[0] * g.Nm[1] : 0, (int64_t)C * nm};
         HB_TRY(launch_fft_pass(op, p->fl[2], F * g.Nm[0] * g.Nm[1], C, (int)g.Nm[2], (int)-h2, g.nf[2], 0, inv, 0, s,
                                "type2 axis2"));
     }
@@ -1631,7 +1653,7 @@ int plan_execute(NufftPlan* p, const float2* in, float2* out, cudaStream_t s) {
         // axis 2 -> caller's modes [F][C][Nm..] with deapodisation
         {
             OpModesOut op{cur, out, p->deapod[0], p->deapod[1], p->deapod[2], g.Nm[1], g.Nm[2], nm,
-                          (int64_t)g.nf[2] * C, C, g.Nm[0] * g.Nm[1], (int64_t)C * nm};
+                          (int64_t)g.nf[2] * C, C, F > 1 ? g.Nm[0] * g.Nm[1] : 0, (int64_t)C * nm};
             HB_TRY(launch_fft_pass(op, p->fl[2], F * g.Nm[0] * g.Nm[1], C, g.nf[2], 0, (int)g.Nm[2], (int)-h2, inv, 0, s,
                                    "type1 axis2"));
         }
