@@ -194,16 +194,15 @@ constexpr int max_kcols() {
 // the input / output of an operator without a fixed shape (kHalfIO 0): the launcher picks them
 // from the pass's lengths and shifts.
 //
-// CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (95 registers; at 64 it spills
-// and runs slower; prefetching the next chunk, 160^3 x 32 coils: 0.875 against 0.957 ms), the
-// prefetching fused-kernel pass at L = 320 2 (96 registers: its samples arrive by cp.async while
-// the previous block is transformed, 3.66 against 4.03 ms; at 3 CTAs, 64 registers, it spills 328
-// bytes per thread and runs 22 % slower), other fused-kernel passes 3, every other pass 4 (48
+// CTAs per SM (320-thread blocks): the coil-reduce pass keeps 2 (96 registers; prefetching the
+// next chunk, 160^3 x 32 coils: 0.756 ms; at 3 CTAs it spills 32 bytes per thread and takes
+// 0.805 ms), the fused-kernel passes 3 (64 registers; the prefetching instance at L = 320 spills
+// 12 bytes and takes 3.31 ms against 3.41 ms at 2 CTAs and 96 registers), every other pass 4 (48
 // registers, a few spilled words): they move bytes, and the fourth CTA hides more of the load
 // latency than the spills cost (prefetching them at 2 or 3 CTAs measured slower).
 template <class Op, int L, int HM, bool PF>
 constexpr int pass2_min_blocks() {
-    return Op::kSenseReduce ? 2 : Op::kFusedK ? ((PF && L == 320) ? 2 : 3) : (PF ? ((HM & 1) ? 3 : 2) : 4);
+    return Op::kSenseReduce ? 2 : Op::kFusedK ? 3 : (PF ? ((HM & 1) ? 3 : 2) : 4);
 }
 template <int P, int Q, class Op, int HM = 0, bool PF = false>
 __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks<Op, P * Q, HM, PF>())
@@ -510,9 +509,9 @@ __global__ void __launch_bounds__(Q* kCW, (Q * kCW > 320) ? 1 : pass2_min_blocks
         if constexpr (Op::kFusedK) {
             // multiply by the kernel at position k1 + P k2, inverse Q-point DFT over k2. The thread
             // writes back into the transpose slots it read, so no barrier is needed here; the
-            // one-CTA-per-block instances (64 registers) keep one as a scheduling fence (without
-            // it the compiler interleaves the two halves and spills). The prefetching instances
-            // (96 registers) run without it: 3.39 against 3.51 ms for P3 at 160^3 x 32 coils.
+            // one-CTA-per-block instances keep one as a scheduling fence (without it the compiler
+            // interleaves the two halves and spills). The prefetching instances run without it
+            // (3.39 against 3.51 ms for P3 at 160^3 x 32 coils, measured at 2 CTAs per SM).
             if (!PF) __syncthreads();
             if (s2active) {
                 if (k_staged) {

@@ -10,9 +10,10 @@
 // double-buffered chunks: per point the CC values (cp.async) and its tile-relative weight rows
 // along z, y and x (the kernel taps at the cells the footprint covers, zero elsewhere), so a
 // visit multiplies whole rows with no per-cell range or index logic. A warp visits only the points
-// whose footprint meets its block (ballots per 32 candidates, one per half of the block's 8 x
+// whose footprint meets its block (ballots per 32 candidates, one per quarter of the block's 8 x
 // cells). For a visited point every lane forms its 4 row products u_r = w_z w_y v and adds
-// w_x[x] u_r to the 4 x 4 cells of each half of the block that the footprint touches.
+// w_x[x] u_r to the 4 x 2 cells of each quarter of the block that the footprint touches (the
+// multiply-adds of the other quarters would add zero weights).
 //
 // Dense tiles (more candidates than a subproblem holds, maxp) are spread in ceil(total / maxp)
 // parts, one CTA each, however many that is, so the k-space centre of radial and spiral
@@ -67,6 +68,19 @@ __device__ __forceinline__ void lc_half(float (&ar)[4][8], float (&ai)[4][8], co
             ar[r][X0 + x] = fmaf(w[x], ur[r], ar[r][X0 + x]);
             ai[r][X0 + x] = fmaf(w[x], ui[r], ai[r][X0 + x]);
         }
+    }
+}
+
+// acc[r][X0 + x] += w_x * u_r, x < 2 (a quarter of the block's 8 cells)
+template <int X0>
+__device__ __forceinline__ void lc_quarter(float (&ar)[4][8], float (&ai)[4][8], const float w0, const float w1,
+                                           const float (&ur)[4], const float (&ui)[4]) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        ar[r][X0] = fmaf(w0, ur[r], ar[r][X0]);
+        ai[r][X0] = fmaf(w0, ui[r], ai[r][X0]);
+        ar[r][X0 + 1] = fmaf(w1, ur[r], ar[r][X0 + 1]);
+        ai[r][X0 + 1] = fmaf(w1, ui[r], ai[r][X0 + 1]);
     }
 }
 
@@ -291,17 +305,21 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
                 const int* brel = reinterpret_cast<const int*>(bwt + S::kLcChunk * S::kRec);
                 for (int q0 = 0; q0 < n; q0 += 32) {
                     const int qq = q0 + lane;
-                    bool h0 = false, h1 = false;
+                    bool h0 = false, h1 = false, h2 = false, h3 = false;
                     if (qq < n) {
                         const int pk = brel[qq];
                         const int rz = (pk & 0xff) - 16, ry = ((pk >> 8) & 0xff) - 16, rx = ((pk >> 16) & 0xff) - 16;
                         const bool zy = rz <= z0 + S::RZ - 1 && rz + WZ - 1 >= z0 && ry <= y0w + S::G * S::RY - 1 &&
                                         ry + W - 1 >= y0w;
-                        h0 = zy && rx <= x0 + 3 && rx + W - 1 >= x0;
-                        h1 = zy && rx <= x0 + 7 && rx + W - 1 >= x0 + 4;
+                        // the quarters of the block's 8 x cells the footprint rx .. rx+W-1 covers
+                        h0 = zy && rx <= x0 + 1 && rx + W - 1 >= x0;
+                        h1 = zy && rx <= x0 + 3 && rx + W - 1 >= x0 + 2;
+                        h2 = zy && rx <= x0 + 5 && rx + W - 1 >= x0 + 4;
+                        h3 = zy && rx <= x0 + 7 && rx + W - 1 >= x0 + 6;
                     }
                     const unsigned m0 = __ballot_sync(0xffffffffu, h0), m1 = __ballot_sync(0xffffffffu, h1);
-                    unsigned bits = m0 | m1;
+                    const unsigned m2 = __ballot_sync(0xffffffffu, h2), m3 = __ballot_sync(0xffffffffu, h3);
+                    unsigned bits = m0 | m1 | m2 | m3;
                     // visits two at a time: both points' loads and row products are issued before
                     // either's multiply-adds, so one visit's shared-memory latency hides behind the
                     // other's arithmetic
@@ -315,11 +333,16 @@ __global__ void __launch_bounds__(LcShape<CC, D3>::THREADS)
                         float4 xa0, xa1, xb0, xb1;
                         lc_prep<CC, D3>(bval, bwt, q0 + ia, coil, z0, y0g, x0, ura, uia, xa0, xa1);
                         lc_prep<CC, D3>(bval, bwt, q0 + ib, coil, z0, y0g, x0, urb, uib, xb0, xb1);
-                        if ((m0 >> ia) & 1u) lc_half<0>(ar, ai, xa0, ura, uia);
-                        if ((m1 >> ia) & 1u) lc_half<4>(ar, ai, xa1, ura, uia);
+                        // only the quarters the footprint covers (the others would add zero weights)
+                        if ((m0 >> ia) & 1u) lc_quarter<0>(ar, ai, xa0.x, xa0.y, ura, uia);
+                        if ((m1 >> ia) & 1u) lc_quarter<2>(ar, ai, xa0.z, xa0.w, ura, uia);
+                        if ((m2 >> ia) & 1u) lc_quarter<4>(ar, ai, xa1.x, xa1.y, ura, uia);
+                        if ((m3 >> ia) & 1u) lc_quarter<6>(ar, ai, xa1.z, xa1.w, ura, uia);
                         if (two) {
-                            if ((m0 >> ib) & 1u) lc_half<0>(ar, ai, xb0, urb, uib);
-                            if ((m1 >> ib) & 1u) lc_half<4>(ar, ai, xb1, urb, uib);
+                            if ((m0 >> ib) & 1u) lc_quarter<0>(ar, ai, xb0.x, xb0.y, urb, uib);
+                            if ((m1 >> ib) & 1u) lc_quarter<2>(ar, ai, xb0.z, xb0.w, urb, uib);
+                            if ((m2 >> ib) & 1u) lc_quarter<4>(ar, ai, xb1.x, xb1.y, urb, uib);
+                            if ((m3 >> ib) & 1u) lc_quarter<6>(ar, ai, xb1.z, xb1.w, urb, uib);
                         }
                     }
                 }
