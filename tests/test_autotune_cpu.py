@@ -98,3 +98,17 @@ def test_interp_choice_is_cached_apart_from_spreading(tmp_path, monkeypatch):
     calls.clear()
     autotune.apply(FakePlan(), dict(spread, **got))
     assert calls == [("kernel", "cells"), ("tuning", 1024, (2, 4, 4)), ("interp", 4)]
+
+
+def test_cache_key_separates_trajectory_families():
+    """Radial spokes, cones spirals and uniform random points with the same point count and
+    problem get different keys (a choice tuned on one family is not reused for another), while a
+    re-drawn trajectory of the same family reuses it."""
+    from hastycucompute_b200 import synthetic
+    radial = [torch.from_numpy(np.ascontiguousarray(c)) for c in synthetic.golden_means_radial(256, 128)]
+    cones = [torch.from_numpy(np.ascontiguousarray(c)) for c in synthetic.cones_spiral(128, 256)]
+    uniform = _coords(32768)
+    keys = {autotune._key((32, 32, 32), 8, 6, c) for c in (radial, cones, uniform)}
+    assert len(keys) == 3
+    radial2 = [torch.from_numpy(np.ascontiguousarray(c)) for c in synthetic.golden_means_radial(256, 128, offset=256)]
+    assert autotune._key((32, 32, 32), 8, 6, radial2) == autotune._key((32, 32, 32), 8, 6, radial)
