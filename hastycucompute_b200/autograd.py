@@ -24,10 +24,12 @@ from .nufft import NufftOpts, NufftPlan, NufftType
 
 
 def coord_grad(plan2: NufftPlan, modes: torch.Tensor, h: torch.Tensor) -> torch.Tensor:
-    """hb_nufft_coord_grad: [dim, M] float32 gradient for the points of type-2 `plan2`."""
+    """hb_nufft_coord_grad: [dim, M] float32 gradient for the points of type-2 `plan2` (a plan set
+    with ``setpts_frames`` takes frame-stacked modes [F, ntransf, N..] and gives every frame's
+    points' gradients back to back along M)."""
     modes = modes.contiguous()
     h = h.contiguous()
-    check_tensor(modes, "modes", torch.complex64, (plan2.ntransf, *plan2.nmodes), plan2.device)
+    check_tensor(modes, "modes", torch.complex64, plan2._mode_shape(), plan2.device)
     check_tensor(h, "h", torch.complex64, (plan2.ntransf, plan2.M), plan2.device)
     grad = torch.empty((plan2.dim, plan2.M), dtype=torch.float32, device=plan2.device)
     _lib.call("hb_nufft_coord_grad", plan2._h, ptr(modes), ptr(h), ptr(grad), stream_ptr(plan2.device))

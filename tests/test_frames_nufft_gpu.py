@@ -177,3 +177,26 @@ def test_batched_sense_op_matches_oracle_per_frame(cuda):
         y = gridding.nufft2(fr[f], S * x[f][None], w=w)
         ref = (np.conj(S) * gridding.nufft1(fr[f], y, shape, w=w)).sum(0)
         assert relerr(got[f], ref) <= PARITY, f"frame {f}"
+
+
+@pytest.mark.gpu
+def test_frames_coordinate_gradient(cuda):
+    """The coordinate gradient of a frame-batched type-2 plan equals each frame's own."""
+    import hastycucompute_b200 as hb
+    from hastycucompute_b200.autograd import coord_grad
+    rng = np.random.default_rng(17)
+    nmodes, T, w, counts = (12, 16, 14), 4, 6, (1500, 0, 2600)
+    fr = _frames(rng, 3, counts)
+    modes = crand(rng, len(counts), T, *nmodes)
+    h = crand(rng, T, sum(counts))
+    plan = _plan(hb, hb.NufftType.TYPE_2, nmodes, T, w)
+    plan.setpts_frames([[to_dev(x, cuda) for x in f] for f in fr])
+    got = to_np(coord_grad(plan, to_dev(modes, cuda), to_dev(h, cuda)))
+    single = _plan(hb, hb.NufftType.TYPE_2, nmodes, T, w)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    for f, m in enumerate(counts):
+        if m == 0:
+            continue
+        single.setpts([to_dev(x, cuda) for x in fr[f]])
+        one = to_np(coord_grad(single, to_dev(modes[f], cuda), to_dev(np.ascontiguousarray(h[:, off[f]: off[f + 1]]), cuda)))
+        assert relerr(got[:, off[f]: off[f + 1]], one) <= 1e-6, f"frame {f}"
