@@ -227,11 +227,44 @@ __global__ void k_tile_extra_count(const int* bin_start, TileNbr t, int64_t ntil
     extra_cnt[tile] = (int)(nsub - 1);
 }
 
-__global__ void k_tile_extra_fill(const int* extra_cnt, const int* extra_off, int64_t ntiles, int2* extra) {
+__global__ void k_tile_extra_fill(const int* extra_cnt, const int* extra_off, int64_t ntiles, int4* extra) {
     const int64_t tile = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tile >= ntiles) return;
     const int n = extra_cnt[tile], off = extra_off[tile];
-    for (int c = 0; c < n; ++c) extra[off + c] = make_int2((int)tile, c + 1);
+    for (int c = 0; c < n; ++c) extra[off + c] = make_int4((int)tile, c + 1, n, off);
+}
+
+// Adds the extra subproblems' partial tiles into the grid: CTA blockIdx.x takes entry e = extra[b]
+// and, for its share (chunk e.y - 1 of e.z) of the tile's cells x transforms, adds the tile's e.z
+// scratch slots e.w .. e.w + e.z - 1 in slot order to the grid value chunk 0 stored. Deterministic:
+// no atomics, a fixed sum order.
+__global__ void __launch_bounds__(256) k_spread_extra_reduce(const GridArgs a) {
+    const GridGeom& g = a.g;
+    const int4 e = a.extra[blockIdx.x];
+    int tile = e.x;
+    const int fr = split_frame_tile(g, tile);
+    float2* const gridf = a.grid + fr * g.fgrid;
+    const int T0 = g.T[0], T1 = g.T[1], T2 = g.T[2];
+    const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
+    const int org0 = tz * T0, org1 = ty * T1, org2 = tx * T2;
+    const int64_t E = (int64_t)T0 * T1 * T2 * g.C;
+    const int q = e.y - 1, n = e.z;
+    const int64_t i0 = q * E / n, i1 = (q + 1) * E / n;
+    const float2* src = a.extra_scratch + (int64_t)e.w * E;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        float2 sum = src[i];
+        for (int s = 1; s < n; ++s) {
+            const float2 v = src[(int64_t)s * E + i];
+            sum.x += v.x;
+            sum.y += v.y;
+        }
+        const int64_t cell = i / g.C;
+        const int c = (int)(i - cell * g.C);
+        const int x = (int)(cell % T2), y = (int)((cell / T2) % T1), z = (int)(cell / ((int64_t)T2 * T1));
+        float2* dst = gridf + (((int64_t)(org0 + z) * g.nf[1] + (org1 + y)) * g.nf[2] + org2 + x) * g.C + c;
+        const float2 v0 = *dst;
+        *dst = make_float2(v0.x + sum.x, v0.y + sum.y);
+    }
 }
 
 // Dense tiles (more candidates than a subproblem holds) for the lanes-on-transforms kernel: a
@@ -330,7 +363,7 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
 
     int tile, chunk;
     if (extra_mode) {
-        const int2 e = a.extra[blockIdx.x];
+        const int4 e = a.extra[blockIdx.x];
         tile = e.x;
         chunk = e.y;
     } else {
@@ -340,6 +373,8 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
     const int fr = split_frame_tile(g, tile);
     const int fbin = fr * (int)g.ntf;
     float2* const gridf = a.grid + fr * g.fgrid;
+    // an extra subproblem writes its partial tile [cell][C] to its scratch slot
+    float2* const xslot = extra_mode ? a.extra_scratch + (int64_t)blockIdx.x * cells * g.C : nullptr;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int o0 = tz * T0, o1 = ty * T1, o2 = tx * T2;
 
@@ -421,13 +456,8 @@ __global__ void __launch_bounds__(kGridThreads) k_spread(const GridArgs a, int e
             if (cc0 + c >= g.C) continue;
             const int cx = cell % T2, cy = (cell / T2) % T1, cz = cell / (T1 * T2);
             const int64_t gi = ((int64_t)(o0 + cz) * g.nf[1] + (o1 + cy)) * g.nf[2] + (o2 + cx);
-            float2* dst = gridf + gi * g.C + cc0 + c;
-            if (extra_mode) {
-                atomicAdd(&dst->x, acc_re[i]);
-                atomicAdd(&dst->y, acc_im[i]);
-            } else {
-                *dst = make_float2(acc_re[i], acc_im[i]);
-            }
+            float2* dst = extra_mode ? xslot + (int64_t)cell * g.C + cc0 + c : gridf + gi * g.C + cc0 + c;
+            *dst = make_float2(acc_re[i], acc_im[i]);
         }
         __syncthreads();
     }
@@ -482,7 +512,7 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
 
     int tile, chunk;
     if (extra_mode) {
-        const int2 e = a.extra[blockIdx.x];
+        const int4 e = a.extra[blockIdx.x];
         tile = e.x;
         chunk = e.y;
     } else {
@@ -492,6 +522,8 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
     const int fr = split_frame_tile(g, tile);
     const int fbin = fr * (int)g.ntf;
     float2* const gridf = a.grid + fr * g.fgrid;
+    // an extra subproblem writes its partial tile [cell][C] to its scratch slot
+    float2* const slot = extra_mode ? a.extra_scratch + (int64_t)blockIdx.x * (T0 * T1 * T2) * g.C : nullptr;
     const int tx = tile % g.nb[2], ty = (tile / g.nb[2]) % g.nb[1], tz = tile / (g.nb[2] * g.nb[1]);
     const int org0 = tz * T0, org1 = ty * T1, org2 = tx * T2;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -723,13 +755,13 @@ __global__ void __launch_bounds__(kSpreadThreads, (CC <= 8) ? 2 : 1)
                     const int jy = (byi << lby) + ((j >> lbx) & (wb.by - 1));
                     const int jx = (bxi << lbx) + (j & (wb.bx - 1));
                     if (cg < g.C) {
-                        const int64_t gi = ((int64_t)(org0 + jz) * nf1 + (org1 + jy)) * nf2 + (org2 + jx);
                         const float2 v = ow[j * (H + 1) + c];
-                        float2* dst = gridf + gi * g.C + cg;
-                        if (extra_mode)
-                            atomicAdd(dst, v);
-                        else
-                            *dst = v;
+                        if (extra_mode) {
+                            slot[((int64_t)(jz * T1 + jy) * T2 + jx) * g.C + cg] = v;
+                        } else {
+                            const int64_t gi = ((int64_t)(org0 + jz) * nf1 + (org1 + jy)) * nf2 + (org2 + jx);
+                            gridf[gi * g.C + cg] = v;
+                        }
                     }
                 }
                 __syncwarp();
@@ -1445,8 +1477,17 @@ int plan_setpts_frames(NufftPlan* p, int nframes, const int64_t* npts, const flo
             if (n_extra > p->extra_cap) {
                 if (p->extra) cudaFree(p->extra);
                 p->extra = nullptr;
-                if ((st = dev_alloc(p, (void**)&p->extra, sizeof(int2) * n_extra, "spread work list")) != HB_OK) break;
+                p->extra_cap = 0;
+                if ((st = dev_alloc(p, (void**)&p->extra, sizeof(int4) * n_extra, "spread work list")) != HB_OK) break;
                 p->extra_cap = n_extra;
+            }
+            const size_t need = sizeof(float2) * (size_t)n_extra * g.T[0] * g.T[1] * g.T[2] * g.C;
+            if (need > p->extra_scratch_cap) {
+                if (p->extra_scratch) cudaFree(p->extra_scratch);
+                p->extra_scratch = nullptr;
+                p->extra_scratch_cap = 0;
+                if ((st = dev_alloc(p, (void**)&p->extra_scratch, need, "spread partial tiles")) != HB_OK) break;
+                p->extra_scratch_cap = need;
             }
             p->n_extra = n_extra;
             if (n_extra > 0) {
@@ -1485,6 +1526,7 @@ static GridArgs grid_args(const NufftPlan* p) {
     a.inT = p->inT;
     a.grid = p->X;
     a.extra = p->extra;
+    a.extra_scratch = p->extra_scratch;
     a.maxp = p->maxp;
     a.kb = p->kb;
     return a;
@@ -1508,6 +1550,8 @@ static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t 
             TimedSection ts("spread_dense", s);
             k_spread_reg<CC><<<(unsigned)p->n_extra, kSpreadThreads, smem, s>>>(a, 1, wb);
             HB_TRY(check_launch("k_spread_reg(extra)"));
+            k_spread_extra_reduce<<<(unsigned)p->n_extra, 256, 0, s>>>(a);
+            HB_TRY(check_launch("k_spread_extra_reduce"));
         }
         return HB_OK;
     }
@@ -1522,6 +1566,8 @@ static int launch_spread_cc(const NufftPlan* p, const GridArgs& a, cudaStream_t 
         TimedSection ts("spread_dense", s);
         k_spread<CC><<<(unsigned)p->n_extra, kGridThreads, smem, s>>>(a, 1);
         HB_TRY(check_launch("k_spread(extra)"));
+        k_spread_extra_reduce<<<(unsigned)p->n_extra, 256, 0, s>>>(a);
+        HB_TRY(check_launch("k_spread_extra_reduce"));
     }
     return HB_OK;
 }
@@ -1791,6 +1837,8 @@ void plan_free(NufftPlan* p) {
     if (p->inT) cudaFree(p->inT);
     if (p->bin_start) cudaFree(p->bin_start);
     if (p->extra) cudaFree(p->extra);
+    if (p->extra_scratch) cudaFree(p->extra_scratch);
+    p->extra_scratch = nullptr;
     if (p->d_err) cudaFree(p->d_err);
     for (int ax = 0; ax < 3; ++ax) {
         if (p->tmp_u[ax]) cudaFree(p->tmp_u[ax]);

@@ -55,9 +55,14 @@ struct NufftPlan {
     float2* inT = nullptr;  // type 1: [M][C] input with the transforms interleaved (caller point order)
     int* bin_start = nullptr;
     int64_t nbins = 0;
-    int2* extra = nullptr;  // spread subproblems beyond the first chunk of each tile
+    // spread subproblems beyond the first chunk of each tile ({tile, chunk, extra chunks of the
+    // tile, first entry of the tile}); each writes its partial tile to its scratch slot (slot =
+    // entry), and a reduction adds a tile's slots into the grid in slot order
+    int4* extra = nullptr;
     int64_t n_extra = 0;
     int64_t extra_cap = 0;
+    float2* extra_scratch = nullptr;
+    size_t extra_scratch_cap = 0;  // bytes
     int* d_err = nullptr;
     bool pts_set = false;
     // frames: grids are allocated for frames_cap frames; foff holds the current frames' point
@@ -114,7 +119,8 @@ struct GridArgs {
     float2* grid;       // [nf0][nf1][nf2][C]
     float2* out;        // interp output [C][M]
     const int* foff;    // frame point offsets [nfr + 1] (nullptr with one frame)
-    const int2* extra;
+    const int4* extra;
+    float2* extra_scratch;  // [entry][tile cell][C] partial tiles of the extra subproblems
     int maxp;
     KbPoly kb;
 };
