@@ -121,3 +121,19 @@ def test_multiplication_rejects_bad_flags_before_touching_the_device():
         st = lib.hb_toeplitz_multiplication(3, shp, 1, dummy, dummy, dummy, dummy, 1 << 30, None, None, *flags, None)
         assert st == 1, (bad, lib.hb_last_error())
         assert b"Invalid" in lib.hb_last_error()
+
+
+def test_frame_entry_points_reject_bad_arguments_before_touching_the_device():
+    """hb_nufft_setpts_frames and hb_toeplitz_kernels_frames check their host arguments first."""
+    from hastycucompute_b200 import _lib
+    lib = _lib.load()
+    npts = _lib.i64_array([100, 0, 50])
+    dummy = C.c_void_p(16)
+    assert lib.hb_nufft_setpts_frames(None, 3, npts, dummy, dummy, dummy, None) == 1
+    assert b"plan" in lib.hb_last_error()
+    kshape = _lib.i64_array([16, 16, 16])
+    assert lib.hb_toeplitz_kernels_frames(4, kshape, 3, npts, dummy, dummy, dummy, dummy, dummy, 6, None) == 1
+    assert lib.hb_toeplitz_kernels_frames(3, kshape, 0, npts, dummy, dummy, dummy, dummy, dummy, 6, None) == 1
+    assert lib.hb_toeplitz_kernels_frames(3, kshape, 3, None, dummy, dummy, dummy, dummy, dummy, 6, None) == 1
+    assert lib.hb_toeplitz_kernels_frames(3, _lib.i64_array([16, 15, 16]), 3, npts, dummy, dummy, dummy, dummy, dummy,
+                                          6, None) == 2
